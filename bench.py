@@ -1,0 +1,449 @@
+#!/usr/bin/env python
+"""Benchmark of the KPM moment loop (the LSQT hot path) on B200.
+
+One step = one KPM moment set: mu_m = <phi|T_m(H/E_max)|phi>, m < 3000, over the
+honeycomb graphene lattice of 2,097,152 sites (4-orbital cell x 1024x512, t = -2.7 eV,
+Anderson W = 1.0 eV, seed 3, E_max 8.7 eV) for one random-phase vector per GPU, in the
+plain FP64 form (the reference's arithmetic). value = site-moments/s over all ranks
+(sites x moments x steps / max-over-ranks device time).
+
+Also reported: the roofline of the dominant kernel (the fused Chebyshev step + moment
+partial sums), the same metric end to end through the public API with host buffers
+(e2e), the FP32-storage batched form (16 vectors per launch) with its DOS error
+against FP64, the Bessel evolution cost, and the reference's CPU path timed on this
+host's cores (cpu_baseline).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Multi-GPU runs are launched with torchrun, one rank per GPU (independent replicas).
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "KPM site-moments/s + HBM GB/s: batched FP32/FP64-acc vs plain FP64 at ≤1e-6 err"
+UNIT = "site-moments/s"
+WORKLOAD = "graphene2m"
+# Algorithmic bytes per site-moment of the fused step (uniform rows, z = 3): ELL index
+# 4 B + complex hopping 16 B per neighbour, on-site potential 8 B, and four complex
+# vector streams (T_{m-2} read, T_{m-1} read once, T_m write, left read).
+Z = 3
+
+
+def fp64_bytes_per_site(z=Z):
+    return z * (4 + 16) + 8 + 4 * 16
+
+
+def fp32_bytes_per_site_vector(V, z=Z):
+    return (z * (4 + 16) + 8) / V + 4 * 8
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ----------------------------------------------------------------------------- plumbing
+def dist():
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                              device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as td
+        td.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as td
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    td.all_reduce(t, op=td.ReduceOp.MAX)
+    return float(t.item())
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during a timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.index), "-f", self.path],
+                stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) >= 9:
+                    rows.append(p)
+        os.remove(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- CPU side
+def reference_dir(src, dst):
+    """A copy of an input directory the reference binaries accept (no seed keywords)."""
+    os.makedirs(dst, exist_ok=True)
+    for f in os.listdir(src):
+        if f.endswith(".in"):
+            shutil.copy(os.path.join(src, f), dst)
+    with open(os.path.join(src, "para.in")) as f:
+        lines = [l for l in f if l.split() and l.split()[0] not in
+                 ("seed", "disorder_seed", "phase_seed")]
+    with open(os.path.join(dst, "para.in"), "w") as f:
+        f.writelines(lines)
+    return dst
+
+
+def host_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def time_reference(ref_dir, n_moments, reps, procs):
+    """Run the reference's find_moments_chebyshev (oracle/_ref/ref_driver) in `procs`
+    independent processes at once; returns per-rep max-over-process seconds."""
+    import oracle
+    if not oracle.have_ref():
+        return None, "reference build oracle/_ref not present"
+    ps = [subprocess.Popen([oracle.REF_DRIVER, "time", ref_dir, str(n_moments), str(reps)],
+                           stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+          for _ in range(procs)]
+    per = []
+    for p in ps:
+        out, _ = p.communicate()
+        if p.returncode != 0:
+            return None, f"ref_driver exited {p.returncode}"
+        per.append(json.loads(out.strip().splitlines()[-1])["reps_s"])
+    return [max(p[r] for p in per) for r in range(reps)], None
+
+
+def cpu_baseline_line(ref_dir, n_sites, n_moments_sample=64, reps=3):
+    procs = min(host_cores(), 64)
+    t, why = time_reference(ref_dir, n_moments_sample, reps, procs)
+    if t is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
+    mean = statistics.mean(t)
+    return {"value": procs * n_sites * n_moments_sample / mean, "unit": UNIT, "cores": procs,
+            "kind": "reference",
+            "sample": f"reference find_moments_chebyshev (oracle/_ref, g++ -O3, serial) on "
+                      f"the same lattice (its fixed seed 12345678), {n_moments_sample} "
+                      f"moments per call, {procs} independent processes at once, "
+                      f"{reps} calls each, mean of the slowest process"}
+
+
+# ----------------------------------------------------------------------------- arms
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from gpuqt_b200 import workloads as W
+    tmp = tempfile.mkdtemp(prefix="gqt_bench_ref_")
+    try:
+        src = W.config_dir(tmp, WORKLOAD)
+        rd = reference_dir(src, os.path.join(tmp, "ref"))
+        n = W.config_sites(WORKLOAD)
+        sample = 64
+        procs = min(host_cores(), 64)
+        t, why = time_reference(rd, sample, args.warmup + args.steps, procs)
+        if t is None:
+            print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+            return
+        timed = t[args.warmup:]
+        mean = statistics.mean(timed)
+        value = procs * n * sample / mean
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": W.CONFIGS[WORKLOAD]["description"] +
+                       f"; bounded sample: {sample} moments per step",
+                       "form": "reference CPU (lsqt_cpu objects), FP64",
+                       "parallelism": f"{procs} host processes (independent vectors)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "sample": f"{sample}-moment find_moments_chebyshev per process "
+                                       f"per step, {procs} processes at once"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def dos_error(g, m, mu64, mu32):
+    e = m.energy
+    d64 = g.chebyshev_summation(mu64[0], mu64[1], e, m.energy_max, m.volume)
+    d32 = g.chebyshev_summation(mu32[0], mu32[1], e, m.energy_max, m.volume)
+    return float(np.max(np.abs(d32 - d64)) / np.max(np.abs(d64)))
+
+
+def run_ours(args):
+    import torch
+
+    import gpuqt_b200 as g
+    from gpuqt_b200 import workloads as W
+
+    rank, world, local = dist()
+    hbm_peak, peak_kind = peaks()
+    tmp = tempfile.mkdtemp(prefix=f"gqt_bench_{rank}_")
+    try:
+        src = W.config_dir(tmp, WORKLOAD)
+        m = g.Model.load(src)
+        n, M = m.n, m.n_moments
+        # Replicas: rank r runs the r-th random-phase vector of the model's stream.
+        for _ in range(rank):
+            m.initial_state()
+        phi = m.initial_state()
+        H = g.Hamiltonian(m)
+        stream = torch.cuda.current_stream()
+        g.set_stream(stream.cuda_stream)
+        x = g.Vector.from_host(*phi)
+        mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
+
+        # --- plain FP64 moment sets, inputs resident in HBM
+        for _ in range(args.warmup):
+            g.moments_device(H, x, x, M, mu.data_ptr())
+        torch.cuda.synchronize()
+        barrier(world)
+        torch.cuda.synchronize()
+        g.reset_launch_count()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with Clocks(local) as clk:
+            t0.record(stream)
+            for _ in range(args.steps):
+                g.moments_device(H, x, x, M, mu.data_ptr())
+            t1.record(stream)
+            torch.cuda.synchronize()
+        launches = g.launch_count()
+        barrier(world)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(t0.elapsed_time(t1), world)
+        clocks = clk.summary()
+        value = world * n * M * args.steps / (ms / 1e3)
+        per_launch_s = t0.elapsed_time(t1) / 1e3 / (args.steps * M)
+        bpl = fp64_bytes_per_site() * n
+        achieved = bpl / per_launch_s / 1e9
+        traffic = None
+        tp = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tp):
+            with open(tp) as f:
+                traffic = json.load(f).get("k_step_fp64_graphene2m_bytes_per_launch")
+
+        # --- e2e: host phase vector (pinned) -> device, moments -> host, every step
+        re_h = torch.from_numpy(np.ascontiguousarray(phi[0])).pin_memory()
+        im_h = torch.from_numpy(np.ascontiguousarray(phi[1])).pin_memory()
+        for _ in range(2):
+            x.upload_ptr(re_h.data_ptr(), im_h.data_ptr())
+            g.moments(H, x, x, M)
+        barrier(world)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            x.upload_ptr(re_h.data_ptr(), im_h.data_ptr())
+            mr, mi = g.moments(H, x, x, M)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        e2e = {"value": world * n * M * args.steps / (e_ms / 1e3), "unit": UNIT,
+               "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": M * 16}
+
+        forms = None
+        evolution = None
+        if not args.no_forms:
+            forms, evolution = measure_forms(g, torch, m, H, phi, args, stream, hbm_peak)
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            cpu = cpu_baseline_line(reference_dir(src, os.path.join(tmp, "ref")), n)
+
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Anderson lattice, random-phase vectors)",
+                "config": {"workload": W.CONFIGS[WORKLOAD]["description"] +
+                           "; one KPM moment set per step, one random-phase vector per GPU",
+                           "form": "plain FP64 (reference arithmetic)",
+                           "parallelism": f"replicas x{world}",
+                           "l2": "inputs larger than L2 (220 MB touched per Chebyshev step)"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
+                             "unit": "GB/s", "frac": achieved / hbm_peak,
+                             "traffic": traffic, "peak_kind": peak_kind,
+                             "kernel": "k_step<double2,V=1,Z=3,Exact,kCheb,dot>",
+                             "bytes_per_launch": bpl},
+                "cpu_baseline": cpu,
+                "e2e": e2e,
+                "gpu_launches": launches,
+                "clocks": clocks,
+                "forms": forms,
+                "evolution": evolution,
+            }
+            print(json.dumps(line), flush=True)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+        barrier(world)
+        if world > 1:
+            import torch.distributed as td
+            td.destroy_process_group()
+
+
+def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
+    """FP32-storage forms on the same lattice: 1 and 16 vectors per launch, with the
+    DOS error of vector 0 against its FP64 moments; and the Bessel evolution."""
+    n, M = m.n, m.n_moments
+    out = {}
+    ev = lambda: (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+    x64 = g.Vector.from_host(*phi)
+    r64, i64 = g.moments(H, x64, x64, M)
+    fp64_rate = None
+    for V in (1, 16):
+        vecs = [phi] + [m.initial_state() for _ in range(V - 1)]
+        re = np.stack([v[0] for v in vecs])
+        im = np.stack([v[1] for v in vecs])
+        X = g.Vector.from_host(re, im, nvec=V, precision=g.FP32)
+        mu = torch.empty(2 * M * V, dtype=torch.float64, device="cuda")
+        for _ in range(2):
+            g.moments_device(H, X, X, M, mu.data_ptr())
+        reps = max(2, min(args.steps, 5))
+        a, b = ev()
+        a.record(stream)
+        for _ in range(reps):
+            g.moments_device(H, X, X, M, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        s = a.elapsed_time(b) / 1e3
+        rate = V * n * M * reps / s
+        bpl = fp32_bytes_per_site_vector(V) * V * n
+        ach = bpl / (s / (reps * M)) / 1e9
+        r32, i32 = g.moments(H, X, X, M)
+        r32, i32 = np.atleast_2d(r32)[0], np.atleast_2d(i32)[0]
+        out[f"fp32_v{V}"] = {"site_moments_per_s": rate, "vectors_per_launch": V,
+                             "achieved_gbs": ach, "frac": ach / hbm_peak,
+                             "bytes_per_site_moment": fp32_bytes_per_site_vector(V),
+                             "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32, i32))}
+    # FP64 rate from a short timed loop for the ratio
+    mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
+    a, b = ev()
+    a.record(stream)
+    for _ in range(3):
+        g.moments_device(H, x64, x64, M, mu.data_ptr())
+    b.record(stream)
+    torch.cuda.synchronize()
+    fp64_rate = n * M * 3 / (a.elapsed_time(b) / 1e3)
+    for k in out:
+        out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / fp64_rate
+    out["fp64_v1_site_moments_per_s"] = fp64_rate
+    # Bessel evolution of one MSD step (1 fs): evolve and evolvex, FP64.
+    dt = m.time_step[0] * m.energy_max
+    st = x64.clone()
+    g.evolve(H, 1, dt, st)
+    g.evolvex(H, 1, dt, st)
+    a, b = ev()
+    before = g.launch_count()
+    a.record(stream)
+    g.evolve(H, 1, dt, st)
+    b.record(stream)
+    terms = g.launch_count() - before - 2  # apply and the 0/1 term precede the series
+    c, d = ev()
+    c.record(stream)
+    g.evolvex(H, 1, dt, st)
+    d.record(stream)
+    torch.cuda.synchronize()
+    evolution = {"dt_scaled": dt, "bessel_terms": terms, "ms_evolve": a.elapsed_time(b),
+                 "ms_evolvex": c.elapsed_time(d)}
+    return out, evolution
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-forms", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,651 @@
+// Operator and algorithm entry points of the C ABI: apply / commutator / current,
+// the Chebyshev terms, the moment loop (find_moments_chebyshev), evolve, evolvex and
+// the Jackson-damped Chebyshev summation. See include/gpuqt.h.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "gqt_algo.h"
+#include "gqt_forms.h"
+#include "gqt_internal.h"
+
+namespace gqt {
+
+Workspace::~Workspace()
+{
+  for (auto& kv : graphs)
+    cudaGraphExecDestroy(kv.second);
+  for (auto& kv : bufs)
+    for (void* p : kv.second.v)
+      cudaFree(p);
+  cudaFree(acc);
+  cudaFree(dot.partials);
+  cudaFree(dot.counter);
+  cudaFree(mu);
+  if (ev_in)
+    cudaEventDestroy(ev_in);
+  if (ev_out)
+    cudaEventDestroy(ev_out);
+  if (capture_stream)
+    cudaStreamDestroy(capture_stream);
+}
+
+Workspace* new_workspace() { return new Workspace(); }
+
+gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i, void** out)
+{
+  auto& b = ws.bufs[{precision, nvec}];
+  if (b.bytes != bytes) {
+    cudaStreamSynchronize(stream());
+    for (void* p : b.v)
+      cudaFree(p);
+    b.v.clear();
+    b.bytes = bytes;
+  }
+  while ((int)b.v.size() <= i) {
+    void* p = nullptr;
+    GQT_CUDA(cudaMalloc(&p, bytes));
+    b.v.push_back(p);
+  }
+  *out = b.v[i];
+  return GQT_OK;
+}
+
+gqt_status ws_dot(Workspace& ws, int nvec, DotScratch** out)
+{
+  if (!ws.dot.partials) {
+    const int blocks = max_grid();
+    GQT_CUDA(cudaMalloc(&ws.dot.partials, (size_t)blocks * 32 * 4 * sizeof(double)));
+    GQT_CUDA(cudaMalloc(&ws.dot.counter, sizeof(unsigned)));
+    GQT_CUDA(cudaMemset(ws.dot.counter, 0, sizeof(unsigned)));
+    ws.dot.blocks = blocks;
+    ws.dot.nvec = 32;
+  }
+  (void)nvec;
+  *out = &ws.dot;
+  return GQT_OK;
+}
+
+namespace {
+
+Op make_op(const gqt_ham* h)
+{
+  Op op;
+  op.n = h->n;
+  op.z = h->z;
+  op.uniform = h->uniform;
+  op.nn = h->nn;
+  op.nl = h->nl;
+  op.hop = h->hop;
+  op.pot = h->pot;
+  op.xx = h->xx;
+  op.emax = h->energy_max;
+  op.inv_emax = 1.0 / h->energy_max;
+  return op;
+}
+
+gqt_status check_pair(const gqt_ham* h, const gqt_vec* a, const char* what)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "%s: null Hamiltonian", what);
+  if (!a || !a->data)
+    return fail(GQT_ERR_ARG, "%s: null vector", what);
+  if (a->n != h->n)
+    return fail(GQT_ERR_ARG, "%s: vector has %d sites, Hamiltonian %d", what, a->n, h->n);
+  return GQT_OK;
+}
+
+gqt_status check_like(const gqt_vec* a, const gqt_vec* b, const char* what)
+{
+  if (!b || !b->data)
+    return fail(GQT_ERR_ARG, "%s: null vector", what);
+  if (a->n != b->n || a->nvec != b->nvec || a->precision != b->precision)
+    return fail(GQT_ERR_ARG, "%s: vectors differ in size, count or precision", what);
+  return GQT_OK;
+}
+
+const FormOps* ops_for(const gqt_vec* v, const char* what)
+{
+  const FormOps* f = form_ops(v->precision, v->nvec);
+  if (!f)
+    fail(GQT_ERR_ARG, "%s: unsupported vector form", what);
+  return f;
+}
+
+gqt_status check_label(int label, const char* what)
+{
+  if (label < 1 || label > 4)
+    return fail(GQT_ERR_ARG, "%s: label must be 1..4 (got %d)", what, label);
+  return GQT_OK;
+}
+
+gqt_status need_fp64(const gqt_vec* v, const char* what)
+{
+  if (v->precision != GQT_FP64)
+    return fail(GQT_ERR_ARG,
+                "%s: single Chebyshev terms take FP64 vectors; use gqt_evolve/gqt_evolvex "
+                "for the FP32 form",
+                what);
+  return GQT_OK;
+}
+
+// The label of term m of evolve (src/sigma.cu:136-145).
+int evolve_label(int m, int direction)
+{
+  const int r = m % 4;
+  if (r == 0)
+    return 1;
+  if (r == 2)
+    return 2;
+  if ((r == 1 && direction == 1) || (r == 3 && direction == -1))
+    return 3;
+  return 4;
+}
+
+// The label of term m of evolvex (src/sigma.cu:180-190).
+int evolvex_label(int m, int direction)
+{
+  const int r = m % 4;
+  if (r == 1)
+    return 3;
+  if (r == 3)
+    return 4;
+  if ((r == 0 && direction == 1) || (r == 2 && direction == -1))
+    return 1;
+  return 2;
+}
+
+// The launch sequence of the moment loop (src/sigma.cu:33-61) on the current stream.
+// Buffers: T_0 = right (read only), T_1 -> A, then T_m overwrites T_{m-2} in place.
+gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* left,
+                           const gqt_vec* right, int M, double2* mu, void* A, void* B,
+                           DotScratch* ds)
+{
+  const Op op = make_op(h);
+  const int V = right->nvec;
+  const size_t total = (size_t)h->n * V;
+  Dot d{ds->partials, ds->counter, mu};
+  GQT_TRY(f->dot(total, right->data, left->data, d));
+  if (M < 2)
+    return GQT_OK;
+  d.mu = mu + V;
+  GQT_TRY(f->step(op, kApply, nullptr, right->data, A, left->data, &d));
+  const void* prev = right->data;  // T_{m-2}
+  void* cur = A;                   // T_{m-1}
+  for (int m = 2; m < M; ++m) {
+    void* out = (prev == right->data) ? B : (void*)prev;
+    d.mu = mu + (size_t)m * V;
+    GQT_TRY(f->step(op, kCheb, prev, cur, out, left->data, &d));
+    prev = cur;
+    cur = out;
+  }
+  return GQT_OK;
+}
+
+}  // namespace
+
+}  // namespace gqt
+
+using namespace gqt;
+
+// ------------------------------------------------------------------ operators
+extern "C" gqt_status gqt_apply(const gqt_ham* h, const gqt_vec* in, gqt_vec* out)
+{
+  GQT_TRY(check_pair(h, in, "gqt_apply"));
+  GQT_TRY(check_like(in, out, "gqt_apply"));
+  if (in->data == out->data)
+    return fail(GQT_ERR_ARG, "gqt_apply: input and output must differ");
+  const FormOps* f = ops_for(in, "gqt_apply");
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->step(make_op(h), kApply, nullptr, in->data, out->data, nullptr, nullptr);
+}
+
+static gqt_status xop_entry(const gqt_ham* h, const gqt_vec* in, gqt_vec* out, bool current,
+                            const char* what)
+{
+  GQT_TRY(check_pair(h, in, what));
+  GQT_TRY(check_like(in, out, what));
+  if (in->data == out->data)
+    return fail(GQT_ERR_ARG, "%s: input and output must differ", what);
+  if (!h->has_xx)
+    return fail(GQT_ERR_STATE, "%s: the Hamiltonian was created without xx", what);
+  const FormOps* f = ops_for(in, what);
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->xop(make_op(h), current, in->data, out->data);
+}
+
+extern "C" gqt_status gqt_apply_commutator(const gqt_ham* h, const gqt_vec* in, gqt_vec* out)
+{
+  return xop_entry(h, in, out, false, "gqt_apply_commutator");
+}
+
+extern "C" gqt_status gqt_apply_current(const gqt_ham* h, const gqt_vec* in, gqt_vec* out)
+{
+  return xop_entry(h, in, out, true, "gqt_apply_current");
+}
+
+extern "C" gqt_status gqt_kernel_polynomial(const gqt_ham* h, const gqt_vec* s0,
+                                            const gqt_vec* s1, gqt_vec* s2)
+{
+  GQT_TRY(check_pair(h, s1, "gqt_kernel_polynomial"));
+  GQT_TRY(check_like(s1, s0, "gqt_kernel_polynomial"));
+  GQT_TRY(check_like(s1, s2, "gqt_kernel_polynomial"));
+  if (s2->data == s1->data)
+    return fail(GQT_ERR_ARG, "gqt_kernel_polynomial: s2 must not alias s1");
+  const FormOps* f = ops_for(s1, "gqt_kernel_polynomial");
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->step(make_op(h), kCheb, s0->data, s1->data, s2->data, nullptr, nullptr);
+}
+
+extern "C" gqt_status gqt_chebyshev_01(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
+                                       gqt_vec* out, double b0, double b1, int direction)
+{
+  GQT_TRY(check_pair(h, s0, "gqt_chebyshev_01"));
+  GQT_TRY(check_like(s0, s1, "gqt_chebyshev_01"));
+  GQT_TRY(check_like(s0, out, "gqt_chebyshev_01"));
+  GQT_TRY(need_fp64(s0, "gqt_chebyshev_01"));
+  const FormOps* f = ops_for(s0, "gqt_chebyshev_01");
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->cheb01((size_t)s0->n * s0->nvec, s0->data, s1->data, (double2*)out->data, b0,
+                   b1 * direction);
+}
+
+extern "C" gqt_status gqt_chebyshev_2(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
+                                      gqt_vec* s2, gqt_vec* out, double bessel, int label)
+{
+  GQT_TRY(check_pair(h, s1, "gqt_chebyshev_2"));
+  GQT_TRY(check_like(s1, s0, "gqt_chebyshev_2"));
+  GQT_TRY(check_like(s1, s2, "gqt_chebyshev_2"));
+  GQT_TRY(check_like(s1, out, "gqt_chebyshev_2"));
+  GQT_TRY(need_fp64(s1, "gqt_chebyshev_2"));
+  GQT_TRY(check_label(label, "gqt_chebyshev_2"));
+  if (s2->data == s1->data || out->data == s1->data || out->data == s2->data)
+    return fail(GQT_ERR_ARG, "gqt_chebyshev_2: s2/out must not alias s1 or each other");
+  const FormOps* f = ops_for(s1, "gqt_chebyshev_2");
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->cheb2(make_op(h), s0->data, s1->data, s2->data, (double2*)out->data, bessel,
+                  label);
+}
+
+extern "C" gqt_status gqt_chebyshev_1x(const gqt_ham* h, const gqt_vec* in, gqt_vec* out,
+                                       double b1)
+{
+  GQT_TRY(check_pair(h, in, "gqt_chebyshev_1x"));
+  GQT_TRY(check_like(in, out, "gqt_chebyshev_1x"));
+  GQT_TRY(need_fp64(in, "gqt_chebyshev_1x"));
+  const FormOps* f = ops_for(in, "gqt_chebyshev_1x");
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->cheb1x((size_t)in->n * in->nvec, in->data, (double2*)out->data, b1);
+}
+
+extern "C" gqt_status gqt_chebyshev_2x(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s0x,
+                                       const gqt_vec* s1, const gqt_vec* s1x, gqt_vec* s2,
+                                       gqt_vec* s2x, gqt_vec* out, double bessel, int label)
+{
+  const char* w = "gqt_chebyshev_2x";
+  GQT_TRY(check_pair(h, s1, w));
+  for (const gqt_vec* v : {s0, s0x, s1x, (const gqt_vec*)s2, (const gqt_vec*)s2x,
+                           (const gqt_vec*)out})
+    GQT_TRY(check_like(s1, v, w));
+  GQT_TRY(need_fp64(s1, w));
+  GQT_TRY(check_label(label, w));
+  const void* gathered[2] = {s1->data, s1x->data};
+  for (const void* g : gathered)
+    if (s2->data == g || s2x->data == g || out->data == g)
+      return fail(GQT_ERR_ARG, "%s: outputs must not alias s1 or s1x", w);
+  const FormOps* f = ops_for(s1, w);
+  if (!f)
+    return GQT_ERR_ARG;
+  return f->cheb2x(make_op(h), s0->data, s0x->data, s1->data, s1x->data, s2->data, s2x->data,
+                   (double2*)out->data, bessel, label);
+}
+
+// ------------------------------------------------------------------ reductions
+namespace {
+thread_local std::map<int, DotScratch> t_dot;  // per device, for Hamiltonian-free dots
+thread_local std::map<int, double2*> t_mu;
+}  // namespace
+
+extern "C" gqt_status gqt_inner_product(const gqt_vec* state, const gqt_vec* left, double* re,
+                                        double* im)
+{
+  if (!state || !state->data)
+    return fail(GQT_ERR_ARG, "gqt_inner_product: null vector");
+  GQT_TRY(check_like(state, left, "gqt_inner_product"));
+  if (!re || !im)
+    return fail(GQT_ERR_ARG, "gqt_inner_product: null output");
+  const FormOps* f = ops_for(state, "gqt_inner_product");
+  if (!f)
+    return GQT_ERR_ARG;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DotScratch& ds = t_dot[dev];
+  double2*& mu = t_mu[dev];
+  if (!ds.partials) {
+    GQT_CUDA(cudaMalloc(&ds.partials, (size_t)max_grid() * 32 * 4 * sizeof(double)));
+    GQT_CUDA(cudaMalloc(&ds.counter, sizeof(unsigned)));
+    GQT_CUDA(cudaMemset(ds.counter, 0, sizeof(unsigned)));
+    GQT_CUDA(cudaMalloc(&mu, 32 * sizeof(double2)));
+  }
+  Dot d{ds.partials, ds.counter, mu};
+  GQT_TRY(f->dot((size_t)state->n * state->nvec, state->data, left->data, d));
+  std::vector<double2> h(state->nvec);
+  GQT_CUDA(cudaMemcpyAsync(h.data(), mu, sizeof(double2) * state->nvec, cudaMemcpyDeviceToHost,
+                           stream()));
+  GQT_CUDA(cudaStreamSynchronize(stream()));
+  for (int k = 0; k < state->nvec; ++k) {
+    re[k] = h[k].x;
+    im[k] = h[k].y;
+  }
+  return GQT_OK;
+}
+
+static DotScratch* thread_dot()
+{
+  int dev = 0;
+  cudaGetDevice(&dev);
+  DotScratch& ds = t_dot[dev];
+  if (!ds.partials) {
+    if (cudaMalloc(&ds.partials, (size_t)max_grid() * 32 * 4 * sizeof(double)) != cudaSuccess)
+      return nullptr;
+    if (cudaMalloc(&ds.counter, sizeof(unsigned)) != cudaSuccess ||
+        cudaMemset(ds.counter, 0, sizeof(unsigned)) != cudaSuccess)
+      return nullptr;
+  }
+  return &ds;
+}
+
+extern "C" gqt_status gqt_inner_product_into(const gqt_vec* state, const gqt_vec* left,
+                                             gqt_vec* target, int index)
+{
+  const char* w = "gqt_inner_product_into";
+  if (!state || !state->data || !target || !target->data)
+    return fail(GQT_ERR_ARG, "%s: null vector", w);
+  GQT_TRY(check_like(state, left, w));
+  if (state->nvec != 1 || target->nvec != 1 || target->precision != GQT_FP64)
+    return fail(GQT_ERR_ARG, "%s: needs single vectors and an FP64 target", w);
+  if (index < 0 || index >= target->n)
+    return fail(GQT_ERR_ARG, "%s: index %d outside the target (%d)", w, index, target->n);
+  const FormOps* f = ops_for(state, w);
+  if (!f)
+    return GQT_ERR_ARG;
+  DotScratch* ds = thread_dot();
+  if (!ds)
+    return fail(GQT_ERR_ALLOC, "%s: scratch allocation failed", w);
+  Dot d{ds->partials, ds->counter, (double2*)target->data + index};
+  return f->dot((size_t)state->n, state->data, left->data, d);
+}
+
+extern "C" gqt_status gqt_vec_segment_sum(const gqt_vec* in, int segment, int count,
+                                          gqt_vec* out)
+{
+  const char* w = "gqt_vec_segment_sum";
+  if (!in || !in->data || !out || !out->data)
+    return fail(GQT_ERR_ARG, "%s: null vector", w);
+  if (in->precision != GQT_FP64 || out->precision != GQT_FP64 || in->nvec != 1 ||
+      out->nvec != 1)
+    return fail(GQT_ERR_ARG, "%s: needs single FP64 vectors", w);
+  if (segment <= 0 || count <= 0 || (size_t)segment * count > (size_t)in->n || count > out->n)
+    return fail(GQT_ERR_ARG, "%s: segment %d x count %d does not fit", w, segment, count);
+  k_segment_sum<0><<<count, kBlock, 0, stream()>>>((const double2*)in->data, segment,
+                                                   (double2*)out->data);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+// ------------------------------------------------------------------ moments
+static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                                  int M, const FormOps** f, void** A, void** B,
+                                  DotScratch** ds)
+{
+  const char* w = "gqt_moments";
+  GQT_TRY(check_pair(h, right, w));
+  GQT_TRY(check_like(right, left, w));
+  if (M < 1)
+    return fail(GQT_ERR_ARG, "%s: number of moments must be > 0 (got %d)", w, M);
+  *f = ops_for(right, w);
+  if (!*f)
+    return GQT_ERR_ARG;
+  Workspace& ws = *h->ws;
+  const size_t bytes = right->bytes;
+  GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
+  GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
+  GQT_TRY(ws_dot(ws, right->nvec, ds));
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
+                                         const gqt_vec* right, int M, void* mu_dev)
+{
+  const FormOps* f;
+  void *A, *B;
+  DotScratch* ds;
+  GQT_TRY(moments_prepare(h, left, right, M, &f, &A, &B, &ds));
+  if (!mu_dev)
+    return fail(GQT_ERR_ARG, "gqt_moments_device: null output");
+  Workspace& ws = *h->ws;
+  cudaStream_t s = stream();
+
+  // The n_moments launches are captured once per (left, right, M, output, form) and
+  // replayed as one graph launch afterwards.
+  Workspace::GraphKey key{left->data, right->data, M, mu_dev, right->precision, right->nvec};
+  auto it = ws.graphs.find(key);
+  if (it == ws.graphs.end()) {
+    if (!ws.capture_stream) {
+      GQT_CUDA(cudaStreamCreateWithFlags(&ws.capture_stream, cudaStreamNonBlocking));
+      GQT_CUDA(cudaEventCreateWithFlags(&ws.ev_in, cudaEventDisableTiming));
+      GQT_CUDA(cudaEventCreateWithFlags(&ws.ev_out, cudaEventDisableTiming));
+    }
+    cudaStream_t saved = s;
+    gqt_set_stream(ws.capture_stream);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(ws.capture_stream, cudaStreamCaptureModeThreadLocal);
+    gqt_status st = GQT_OK;
+    if (e == cudaSuccess) {
+      const uint64_t before = gqt_launch_count();
+      st = moment_launches(h, f, left, right, M, (double2*)mu_dev, A, B, ds);
+      // Captured launches run later, when the graph is launched.
+      gqt_reset_launch_count();
+      count_launches(before);
+      e = cudaStreamEndCapture(ws.capture_stream, &g);
+    }
+    gqt_set_stream(saved);
+    if (st != GQT_OK) {
+      if (g)
+        cudaGraphDestroy(g);
+      return st;
+    }
+    if (e != cudaSuccess)
+      return cuda_fail(e, "stream capture of the moment loop", __FILE__, __LINE__);
+    cudaGraphExec_t exec = nullptr;
+    e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess)
+      return cuda_fail(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    it = ws.graphs.emplace(key, exec).first;
+  }
+  // The graph runs on the workspace's own stream, ordered after and before the
+  // caller's stream by events (the legacy default stream cannot launch graphs
+  // directly into a capture-compatible order).
+  GQT_CUDA(cudaEventRecord(ws.ev_in, s));
+  GQT_CUDA(cudaStreamWaitEvent(ws.capture_stream, ws.ev_in, 0));
+  GQT_CUDA(cudaGraphLaunch(it->second, ws.capture_stream));
+  count_launches((uint64_t)M);
+  GQT_CUDA(cudaEventRecord(ws.ev_out, ws.capture_stream));
+  GQT_CUDA(cudaStreamWaitEvent(s, ws.ev_out, 0));
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                                  int M, double* mu_re, double* mu_im)
+{
+  if (!mu_re || !mu_im)
+    return fail(GQT_ERR_ARG, "gqt_moments: null output");
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_moments: null Hamiltonian");
+  if (!right)
+    return fail(GQT_ERR_ARG, "gqt_moments: null vector");
+  if (M < 1)
+    return fail(GQT_ERR_ARG, "gqt_moments: number of moments must be > 0 (got %d)", M);
+  Workspace& ws = *h->ws;
+  const int V = right->nvec;
+  const size_t need = (size_t)M * V * sizeof(double2);
+  if (ws.mu_bytes < need) {
+    cudaStreamSynchronize(stream());
+    cudaFree(ws.mu);
+    ws.mu = nullptr;
+    ws.mu_bytes = 0;
+    GQT_CUDA(cudaMalloc(&ws.mu, need));
+    ws.mu_bytes = need;
+    // Graphs keyed on the old buffer can never match again; drop them.
+    for (auto& kv : ws.graphs)
+      cudaGraphExecDestroy(kv.second);
+    ws.graphs.clear();
+  }
+  GQT_TRY(gqt_moments_device(h, left, right, M, ws.mu));
+  std::vector<double2> host((size_t)M * V);
+  GQT_CUDA(cudaMemcpyAsync(host.data(), ws.mu, need, cudaMemcpyDeviceToHost, stream()));
+  GQT_CUDA(cudaStreamSynchronize(stream()));
+  for (int k = 0; k < V; ++k)
+    for (int m = 0; m < M; ++m) {
+      mu_re[(size_t)k * M + m] = host[(size_t)m * V + k].x;
+      mu_im[(size_t)k * M + m] = host[(size_t)m * V + k].y;
+    }
+  return GQT_OK;
+}
+
+// ------------------------------------------------------------------ time evolution
+static gqt_status evolve_common(const gqt_ham* h, int direction, double dt, gqt_vec* state,
+                                bool commutator)
+{
+  const char* w = commutator ? "gqt_evolvex" : "gqt_evolve";
+  GQT_TRY(check_pair(h, state, w));
+  if (direction != 1 && direction != -1)
+    return fail(GQT_ERR_ARG, "%s: direction must be +1 or -1 (got %d)", w, direction);
+  if (commutator && !h->has_xx)
+    return fail(GQT_ERR_STATE, "%s: the Hamiltonian was created without xx", w);
+  const FormOps* f = ops_for(state, w);
+  if (!f)
+    return GQT_ERR_ARG;
+  Workspace& ws = *h->ws;
+  const Op op = make_op(h);
+  const size_t total = (size_t)state->n * state->nvec;
+  const size_t bytes = state->bytes;
+  void *s0, *s1, *s0x = nullptr, *s1x = nullptr;
+  GQT_TRY(ws_vector(ws, state->precision, state->nvec, bytes, 0, &s0));
+  GQT_TRY(ws_vector(ws, state->precision, state->nvec, bytes, 1, &s1));
+  if (commutator) {
+    GQT_TRY(ws_vector(ws, state->precision, state->nvec, bytes, 2, &s0x));
+    GQT_TRY(ws_vector(ws, state->precision, state->nvec, bytes, 3, &s1x));
+  }
+  // The FP64 form accumulates straight into the state; the FP32 form into an FP64
+  // accumulator that is rounded to the state once at the end.
+  double2* out = (double2*)state->data;
+  if (state->precision != GQT_FP64) {
+    const size_t need = total * sizeof(double2);
+    if (ws.acc_bytes < need) {
+      cudaStreamSynchronize(stream());
+      cudaFree(ws.acc);
+      ws.acc = nullptr;
+      ws.acc_bytes = 0;
+      GQT_CUDA(cudaMalloc(&ws.acc, need));
+      ws.acc_bytes = need;
+    }
+    out = ws.acc;
+  }
+  cudaStream_t s = stream();
+  GQT_CUDA(cudaMemcpyAsync(s0, state->data, bytes, cudaMemcpyDeviceToDevice, s));
+  GQT_TRY(f->step(op, kApply, nullptr, state->data, s1, nullptr, nullptr));
+  if (!commutator) {
+    const double b0 = j0(dt);
+    const double b1 = 2.0 * j1(dt);
+    GQT_TRY(f->cheb01(total, s0, s1, out, b0, b1 * direction));
+    for (int m = 2; m < 1000000; ++m) {
+      double bm = jn(m, dt);
+      if (bm < 1.0e-15 && bm > -1.0e-15)
+        break;
+      bm *= 2.0;
+      GQT_TRY(f->cheb2(op, s0, s1, s0, out, bm, evolve_label(m, direction)));
+      std::swap(s0, s1);
+    }
+  } else {
+    GQT_CUDA(cudaMemsetAsync(s0x, 0, bytes, s));
+    GQT_TRY(f->xop(op, false, state->data, s1x));
+    const double b1 = 2.0 * j1(dt);
+    GQT_TRY(f->cheb1x(total, s1x, out, b1));
+    for (int m = 2; m <= 1000000; ++m) {
+      double bm = jn(m, dt);
+      if (bm < 1.0e-15 && bm > -1.0e-15)
+        break;
+      bm *= 2.0;
+      GQT_TRY(f->cheb2x(op, s0, s0x, s1, s1x, s0, s0x, out, bm, evolvex_label(m, direction)));
+      std::swap(s0, s1);
+      std::swap(s0x, s1x);
+    }
+  }
+  if (state->precision != GQT_FP64) {
+    const int grid = grid_for((const void*)k_narrow<float2>, total);
+    k_narrow<float2><<<grid, kBlock, 0, s>>>(total, out, (float2*)state->data);
+    count_launches(1);
+    GQT_CUDA(cudaGetLastError());
+  }
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_evolve(const gqt_ham* h, int direction, double dt_scaled,
+                                 gqt_vec* state)
+{
+  return evolve_common(h, direction, dt_scaled, state, false);
+}
+
+extern "C" gqt_status gqt_evolvex(const gqt_ham* h, int direction, double dt_scaled,
+                                  gqt_vec* state)
+{
+  return evolve_common(h, direction, dt_scaled, state, true);
+}
+
+// ------------------------------------------------------------------ summation (host)
+extern "C" gqt_status gqt_chebyshev_summation(int M, double* mu_re, double* mu_im, int n_energy,
+                                              const double* energy, double energy_max,
+                                              double volume, double* out)
+{
+  if (M < 2)
+    return fail(GQT_ERR_ARG, "gqt_chebyshev_summation: needs at least 2 moments (got %d)", M);
+  if (!mu_re || !mu_im || (!energy && n_energy > 0) || (!out && n_energy > 0))
+    return fail(GQT_ERR_ARG, "gqt_chebyshev_summation: null argument");
+  const double PI = 3.141592653589793;
+  // Jackson damping (src/sigma.cu:76-86).
+  for (int k = 0; k < M; ++k) {
+    const double factor = 1.0 / (M + 1);
+    const double damping =
+      (1 - k * factor) * std::cos(k * PI * factor) + std::sin(k * PI * factor) * factor /
+                                                       std::tan(PI * factor);
+    mu_re[k] *= damping;
+    mu_im[k] *= damping;
+  }
+  // Chebyshev summation (src/sigma.cu:89-110).
+  for (int e = 0; e < n_energy; ++e) {
+    const double es = energy[e] / energy_max;
+    double c0 = 1.0, c1 = es, c2;
+    double temp = mu_re[1] * c1;
+    for (int s2 = 2; s2 < M; ++s2) {
+      c2 = 2.0 * es * c1 - c0;
+      c0 = c1;
+      c1 = c2;
+      temp += mu_re[s2] * c2;
+    }
+    temp *= 2.0;
+    temp += mu_re[0];
+    temp *= 2.0 / (PI * volume);
+    temp /= std::sqrt(1.0 - es * es);
+    out[e] = temp / energy_max;
+  }
+  return GQT_OK;
+}

@@ -1,0 +1,39 @@
+// Algorithm layer: per-Hamiltonian workspace (temporary vectors, moment reduction
+// scratch, cached CUDA graphs of the moment loop).
+#pragma once
+
+#include <map>
+#include <tuple>
+#include <vector>
+
+#include "gqt_internal.h"
+
+namespace gqt {
+
+struct Workspace {
+  // Temporary vectors per (precision, nvec), allocated on first use and reused.
+  struct Bufs {
+    size_t bytes = 0;
+    std::vector<void*> v;
+  };
+  std::map<std::pair<int, int>, Bufs> bufs;
+  double2* acc = nullptr;  // FP64 accumulator of the FP32 form's evolution
+  size_t acc_bytes = 0;
+  DotScratch dot;          // block partials + arrival counter of fused moment launches
+  double2* mu = nullptr;   // device moments for the host-returning entry points
+  size_t mu_bytes = 0;
+  cudaStream_t capture_stream = nullptr;  // used when the caller's stream is the legacy one
+  cudaEvent_t ev_in = nullptr, ev_out = nullptr;
+  // Instantiated moment loops: (left, right, n_moments, mu, precision, nvec).
+  using GraphKey = std::tuple<const void*, const void*, int, void*, int, int>;
+  std::map<GraphKey, cudaGraphExec_t> graphs;
+  ~Workspace();
+};
+
+Workspace* new_workspace();
+
+// The i-th temporary vector of a form (n * nvec elements of elem bytes).
+gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i, void** out);
+gqt_status ws_dot(Workspace& ws, int nvec, DotScratch** out);
+
+}  // namespace gqt

@@ -1,0 +1,55 @@
+// Launch tables: one per arithmetic form (FP64 exact / FP32 storage) and vector-block
+// width V. The algorithm layer (gqt_algo.cu) calls through these so each form's
+// template instantiations live in their own translation unit.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "gqt_internal.h"
+#include "gqt_kernels.cuh"
+
+namespace gqt {
+
+struct FormOps {
+  int precision;
+  int nvec;
+  size_t elem_bytes;  // bytes of one complex vector element
+  // out = H t1 (mode kApply) or 2 H t1 - t0 (kCheb); dot != nullptr fuses <left|out>.
+  gqt_status (*step)(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                     const void* left, const Dot* dot);
+  gqt_status (*dot)(size_t total, const void* state, const void* left, const Dot& dot);
+  gqt_status (*xop)(const Op& op, bool current, const void* in, void* out);
+  // Evolution terms; out is a double2 accumulator (the FP64 state itself, or the
+  // FP32 form's FP64 accumulator).
+  gqt_status (*cheb01)(size_t total, const void* s0, const void* s1, double2* out, double b0,
+                       double b1);
+  gqt_status (*cheb2)(const Op& op, const void* s0, const void* s1, void* s2, double2* out,
+                      double bessel, int label);
+  gqt_status (*cheb1x)(size_t total, const void* s1x, double2* out, double b1);
+  gqt_status (*cheb2x)(const Op& op, const void* s0, const void* s0x, const void* s1,
+                       const void* s1x, void* s2, void* s2x, double2* out, double bessel,
+                       int label);
+  gqt_status (*add)(size_t total, void* dst, const void* src);
+  gqt_status (*apply_sz)(size_t total, int nvec, void* dst, const void* src);
+  gqt_status (*interleave)(int n, int nvec, const double* re, const double* im, void* out);
+  gqt_status (*deinterleave)(int n, int nvec, const void* in, double* re, double* im);
+};
+
+const FormOps* forms_fp64(int nvec);
+const FormOps* forms_fp32(int nvec);
+inline const FormOps* form_ops(int precision, int nvec)
+{
+  if (precision == GQT_FP64)
+    return forms_fp64(nvec);
+  if (precision == GQT_FP32)
+    return forms_fp32(nvec);
+  return nullptr;
+}
+
+// Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
+// at the number of blocks that are resident at once on all SMs.
+int grid_for(const void* kernel, size_t total);
+// Upper bound of grid_for over all kernels (sizes the dot partials).
+int max_grid();
+
+}  // namespace gqt

@@ -1,0 +1,141 @@
+// Template bodies of the launch tables; included by gqt_forms_fp64.cu and
+// gqt_forms_fp32.cu only.
+#pragma once
+
+#include <type_traits>
+
+#include "gqt_forms.h"
+
+namespace gqt {
+
+template <class F>
+gqt_status with_z(int z, F&& f)
+{
+  switch (z) {
+    case 3:
+      return f(std::integral_constant<int, 3>{});
+    case 4:
+      return f(std::integral_constant<int, 4>{});
+    case 6:
+      return f(std::integral_constant<int, 6>{});
+    default:
+      return f(std::integral_constant<int, 0>{});
+  }
+}
+
+template <typename K, typename... Args>
+gqt_status launch(K* kernel, size_t total, Args... args)
+{
+  const int grid = grid_for((const void*)kernel, total);
+  kernel<<<grid, kBlock, 0, stream()>>>(args...);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+template <typename VT2, int V, class A>
+struct FormImpl {
+  static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                         const void* left, const Dot* dot)
+  {
+    const size_t total = (size_t)op.n * V;
+    const VT2* a0 = (const VT2*)t0;
+    const VT2* a1 = (const VT2*)t1;
+    VT2* o = (VT2*)out;
+    const VT2* l = (const VT2*)left;
+    Dot d = dot ? *dot : Dot{nullptr, nullptr, nullptr};
+    return with_z(op.z, [&](auto zc) -> gqt_status {
+      constexpr int Z = decltype(zc)::value;
+      if (mode == kApply) {
+        if (dot)
+          return launch(k_step<VT2, V, Z, A, kApply, true>, total, op, a0, a1, o, l, d);
+        return launch(k_step<VT2, V, Z, A, kApply, false>, total, op, a0, a1, o, l, d);
+      }
+      if (dot)
+        return launch(k_step<VT2, V, Z, A, kCheb, true>, total, op, a0, a1, o, l, d);
+      return launch(k_step<VT2, V, Z, A, kCheb, false>, total, op, a0, a1, o, l, d);
+    });
+  }
+
+  static gqt_status dot(size_t total, const void* state, const void* left, const Dot& d)
+  {
+    return launch(k_dot<VT2, V>, total, total, (const VT2*)state, (const VT2*)left, d);
+  }
+
+  static gqt_status xop(const Op& op, bool current, const void* in, void* out)
+  {
+    const size_t total = (size_t)op.n * V;
+    return with_z(op.z, [&](auto zc) -> gqt_status {
+      constexpr int Z = decltype(zc)::value;
+      if (current)
+        return launch(k_xop<VT2, V, Z, A, true>, total, op, (const VT2*)in, (VT2*)out);
+      return launch(k_xop<VT2, V, Z, A, false>, total, op, (const VT2*)in, (VT2*)out);
+    });
+  }
+
+  static gqt_status cheb01(size_t total, const void* s0, const void* s1, double2* out,
+                           double b0, double b1)
+  {
+    return launch(k_cheb01<VT2, double2, A>, total, total, (const VT2*)s0, (const VT2*)s1,
+                  out, b0, b1);
+  }
+
+  static gqt_status cheb2(const Op& op, const void* s0, const void* s1, void* s2,
+                          double2* out, double bessel, int label)
+  {
+    const size_t total = (size_t)op.n * V;
+    return with_z(op.z, [&](auto zc) -> gqt_status {
+      constexpr int Z = decltype(zc)::value;
+      return launch(k_cheb2<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+                    (const VT2*)s1, (VT2*)s2, out, bessel, label);
+    });
+  }
+
+  static gqt_status cheb1x(size_t total, const void* s1x, double2* out, double b1)
+  {
+    return launch(k_cheb1x<VT2, double2, A>, total, total, (const VT2*)s1x, out, b1);
+  }
+
+  static gqt_status cheb2x(const Op& op, const void* s0, const void* s0x, const void* s1,
+                           const void* s1x, void* s2, void* s2x, double2* out,
+                           double bessel, int label)
+  {
+    const size_t total = (size_t)op.n * V;
+    return with_z(op.z, [&](auto zc) -> gqt_status {
+      constexpr int Z = decltype(zc)::value;
+      return launch(k_cheb2x<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+                    (const VT2*)s0x, (const VT2*)s1, (const VT2*)s1x, (VT2*)s2, (VT2*)s2x,
+                    out, bessel, label);
+    });
+  }
+
+  static gqt_status add(size_t total, void* dst, const void* src)
+  {
+    return launch(k_add<VT2>, total, total, (VT2*)dst, (const VT2*)src);
+  }
+
+  static gqt_status apply_sz(size_t total, int nvec, void* dst, const void* src)
+  {
+    return launch(k_apply_sz<VT2>, total, total, nvec, (VT2*)dst, (const VT2*)src);
+  }
+
+  static gqt_status interleave(int n, int nvec, const double* re, const double* im, void* out)
+  {
+    return launch(k_interleave<VT2>, (size_t)n * nvec, n, nvec, re, im, (VT2*)out);
+  }
+
+  static gqt_status deinterleave(int n, int nvec, const void* in, double* re, double* im)
+  {
+    return launch(k_deinterleave<VT2>, (size_t)n * nvec, n, nvec, (const VT2*)in, re, im);
+  }
+
+  static const FormOps* table(int precision)
+  {
+    static const FormOps t = {precision, V,      sizeof(VT2), step,     dot,      xop,
+                              cheb01,    cheb2,  cheb1x,      cheb2x,   add,      apply_sz,
+                              interleave, deinterleave};
+    return &t;
+  }
+};
+
+}  // namespace gqt

@@ -1,0 +1,79 @@
+// Internal declarations shared by the library's translation units (not installed).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gpuqt.h"
+
+namespace gqt {
+
+// Thread-local error message and stream (see gpuqt.h).
+gqt_status fail(gqt_status code, const char* fmt, ...);
+gqt_status cuda_fail(cudaError_t e, const char* what, const char* file, int line);
+cudaStream_t stream();
+void count_launches(uint64_t k);
+
+// Device properties cached per device.
+struct DeviceInfo {
+  int sms = 0;
+};
+const DeviceInfo& device_info();
+
+// One reduction lane set: per-block partials of one fused launch and the arrival
+// counter of the last-block reduction. All launches on one stream share it, in order.
+struct DotScratch {
+  double* partials = nullptr;  // [blocks][nvec][4] (re_hi, re_lo, im_hi, im_lo)
+  unsigned* counter = nullptr;
+  int blocks = 0;
+  int nvec = 0;
+};
+
+// Temporary vectors and graph cache reused by the algorithm entry points.
+struct Workspace;
+
+}  // namespace gqt
+
+#define GQT_CUDA(call)                                                 \
+  do {                                                                 \
+    cudaError_t e_ = (call);                                           \
+    if (e_ != cudaSuccess)                                             \
+      return gqt::cuda_fail(e_, #call, __FILE__, __LINE__);            \
+  } while (0)
+
+#define GQT_TRY(expr)            \
+  do {                           \
+    gqt_status s_ = (expr);      \
+    if (s_ != GQT_OK)            \
+      return s_;                 \
+  } while (0)
+
+struct gqt_vec {
+  int n = 0;
+  int nvec = 0;
+  int precision = GQT_FP64;
+  void* data = nullptr;  // double2 or float2, [site][vector]
+  size_t bytes = 0;
+  int device = 0;
+};
+
+struct gqt_ham {
+  int n = 0;
+  int z = 0;
+  double energy_max = 1.0;
+  int uniform = 0;  // every row has z entries: neighbor_number is not read
+  int device = 0;
+  int* nn = nullptr;        // [n], null when uniform
+  int* nl = nullptr;        // [z*n] column-major
+  double2* hop = nullptr;   // [z*n] column-major
+  double* xx = nullptr;     // [z*n] column-major
+  double* pot = nullptr;    // [n]
+  bool has_xx = false;
+  std::unique_ptr<gqt::Workspace> ws;
+  ~gqt_ham();
+};

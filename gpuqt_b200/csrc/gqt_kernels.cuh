@@ -1,0 +1,586 @@
+// Device kernels of the LSQT hot path (sm_100a).
+//
+// Every kernel is HBM-bound ELL work: a site reads its row of the column-major ELL
+// arrays (coalesced across a warp), gathers its neighbours' vector values (served
+// mostly from L1/L2 because lattice neighbours are close in index) and streams its
+// own vector entries. Vectors are interleaved complex ([site][vector] double2 or
+// float2), so a gather is one 8- or 16-byte load and V vectors of one site share
+// one ELL row read.
+//
+// Two arithmetic policies:
+//   ExactArith  FP64 with every product, sum and the division by E_max rounded
+//               separately (no FMA contraction), in the order of the reference's
+//               CPU twins (src/hamiltonian.cu:188-221 etc.): per-site results are
+//               bit-identical to the reference.
+//   FastArith   FP64 with FMA for the FP32-storage form: inputs are widened to FP64,
+//               the operator stays FP64, and only the stored vector is rounded.
+//
+// Moments <left|T_m> are fused into the step that produces T_m: each thread keeps
+// compensated (TwoSum) FP64 partial sums, a block combines them with warp shuffles
+// and shared memory, and the last block to finish (arrival counter) combines the
+// block partials in fixed block order. The result does not depend on timing.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+namespace gqt {
+
+constexpr int kBlock = 256;
+
+struct Op {
+  int n;
+  int z;
+  int uniform;
+  const int* __restrict__ nn;
+  const int* __restrict__ nl;
+  const double2* __restrict__ hop;
+  const double* __restrict__ pot;
+  const double* __restrict__ xx;
+  double emax;
+  double inv_emax;
+};
+
+struct Dot {
+  double* partials;  // [gridDim.x][V][4]
+  unsigned* counter;
+  double2* mu;       // this moment's V results
+};
+
+// ------------------------------------------------------------------ arithmetic
+struct ExactArith {
+  static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+  static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+  static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  static __device__ __forceinline__ double scale(double a, const Op& op)
+  {
+    return __ddiv_rn(a, op.emax);
+  }
+  // a*c - b*d and a*d + b*c, each product and sum rounded on its own
+  static __device__ __forceinline__ double cre(double a, double b, double c, double d)
+  {
+    return __dsub_rn(__dmul_rn(a, c), __dmul_rn(b, d));
+  }
+  static __device__ __forceinline__ double cim(double a, double b, double c, double d)
+  {
+    return __dadd_rn(__dmul_rn(a, d), __dmul_rn(b, c));
+  }
+  static __device__ __forceinline__ double two_x_minus(double x, double y)
+  {
+    return __dsub_rn(__dmul_rn(2.0, x), y);
+  }
+};
+
+struct FastArith {
+  static __device__ __forceinline__ double mul(double a, double b) { return a * b; }
+  static __device__ __forceinline__ double add(double a, double b) { return a + b; }
+  static __device__ __forceinline__ double sub(double a, double b) { return a - b; }
+  static __device__ __forceinline__ double scale(double a, const Op& op)
+  {
+    return a * op.inv_emax;
+  }
+  static __device__ __forceinline__ double cre(double a, double b, double c, double d)
+  {
+    return fma(a, c, -b * d);
+  }
+  static __device__ __forceinline__ double cim(double a, double b, double c, double d)
+  {
+    return fma(a, d, b * c);
+  }
+  static __device__ __forceinline__ double two_x_minus(double x, double y)
+  {
+    return fma(2.0, x, -y);
+  }
+};
+
+// ------------------------------------------------------------------ storage
+__device__ __forceinline__ double2 ld(const double2* p) { return *p; }
+__device__ __forceinline__ double2 ld(const float2* p)
+{
+  float2 f = *p;
+  return make_double2((double)f.x, (double)f.y);
+}
+__device__ __forceinline__ void st(double2* p, double2 v) { *p = v; }
+__device__ __forceinline__ void st(float2* p, double2 v)
+{
+  *p = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+}
+// The value a store of v leaves in memory, widened back to FP64.
+__device__ __forceinline__ double2 stored(const double2*, double2 v) { return v; }
+__device__ __forceinline__ double2 stored(const float2*, double2 v)
+{
+  return make_double2((double)__double2float_rn(v.x), (double)__double2float_rn(v.y));
+}
+
+// ------------------------------------------------------------------ compensated sums
+struct CSum {
+  double s, c;
+};
+
+__device__ __forceinline__ void csum_add(CSum& a, double x)
+{
+  double t = __dadd_rn(a.s, x);
+  double z = __dsub_rn(t, a.s);
+  double e = __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, z)), __dsub_rn(x, z));
+  a.s = t;
+  a.c = __dadd_rn(a.c, e);
+}
+
+__device__ __forceinline__ void csum_merge(CSum& a, const CSum& b)
+{
+  double t = __dadd_rn(a.s, b.s);
+  double z = __dsub_rn(t, a.s);
+  double e = __dadd_rn(__dsub_rn(a.s, __dsub_rn(t, z)), __dsub_rn(b.s, z));
+  a.s = t;
+  a.c = __dadd_rn(__dadd_rn(a.c, b.c), e);
+}
+
+// <left|state> term of one element, in the reference's form (src/vector.cu:300-329):
+// re = a*c + b*d, im = b*c - a*d with (a, b) = state and (c, d) = left.
+__device__ __forceinline__ void dot_term(CSum& re, CSum& im, double2 s, double2 l)
+{
+  csum_add(re, __dadd_rn(__dmul_rn(s.x, l.x), __dmul_rn(s.y, l.y)));
+  csum_add(im, __dsub_rn(__dmul_rn(s.y, l.x), __dmul_rn(s.x, l.y)));
+}
+
+__device__ __forceinline__ CSum shfl_xor(const CSum& a, int off)
+{
+  CSum b;
+  b.s = __shfl_xor_sync(0xffffffffu, a.s, off);
+  b.c = __shfl_xor_sync(0xffffffffu, a.c, off);
+  return b;
+}
+
+// Combine the per-thread partials of vector v = lane % V across the block, then
+// across the grid (last block, fixed order), and write dot.mu[v]. Must be reached
+// by every thread of the block.
+template <int V>
+__device__ __forceinline__ void dot_finish(CSum re, CSum im, const Dot& dot)
+{
+  static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two <= 32");
+  constexpr int kWarps = kBlock / 32;
+  __shared__ double sh[kWarps][V][4];
+  __shared__ unsigned is_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+
+#pragma unroll
+  for (int off = 16; off >= V; off >>= 1) {
+    csum_merge(re, shfl_xor(re, off));
+    csum_merge(im, shfl_xor(im, off));
+  }
+  if (lane < V) {
+    sh[warp][lane][0] = re.s;
+    sh[warp][lane][1] = re.c;
+    sh[warp][lane][2] = im.s;
+    sh[warp][lane][3] = im.c;
+  }
+  __syncthreads();
+  if (threadIdx.x < V) {
+    const int v = threadIdx.x;
+    CSum r{sh[0][v][0], sh[0][v][1]}, i{sh[0][v][2], sh[0][v][3]};
+    for (int w = 1; w < kWarps; ++w) {
+      csum_merge(r, CSum{sh[w][v][0], sh[w][v][1]});
+      csum_merge(i, CSum{sh[w][v][2], sh[w][v][3]});
+    }
+    double* p = dot.partials + ((size_t)blockIdx.x * V + v) * 4;
+    p[0] = r.s;
+    p[1] = r.c;
+    p[2] = i.s;
+    p[3] = i.c;
+    __threadfence();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    is_last = (atomicAdd(dot.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
+  __syncthreads();
+  if (!is_last)
+    return;
+  __threadfence();
+
+  // Last block: thread t sums blocks t/V, t/V + kBlock/V, ... of vector t % V.
+  const int v = threadIdx.x % V;
+  CSum r{0.0, 0.0}, i{0.0, 0.0};
+  for (int b = threadIdx.x / V; b < (int)gridDim.x; b += kBlock / V) {
+    const double* p = dot.partials + ((size_t)b * V + v) * 4;
+    csum_merge(r, CSum{__ldcg(p + 0), __ldcg(p + 1)});
+    csum_merge(i, CSum{__ldcg(p + 2), __ldcg(p + 3)});
+  }
+#pragma unroll
+  for (int off = 16; off >= V; off >>= 1) {
+    csum_merge(r, shfl_xor(r, off));
+    csum_merge(i, shfl_xor(i, off));
+  }
+  __syncthreads();
+  if (lane < V) {
+    sh[warp][lane][0] = r.s;
+    sh[warp][lane][1] = r.c;
+    sh[warp][lane][2] = i.s;
+    sh[warp][lane][3] = i.c;
+  }
+  __syncthreads();
+  if (threadIdx.x < V) {
+    CSum rr{sh[0][v][0], sh[0][v][1]}, ii{sh[0][v][2], sh[0][v][3]};
+    for (int w = 1; w < kWarps; ++w) {
+      csum_merge(rr, CSum{sh[w][v][0], sh[w][v][1]});
+      csum_merge(ii, CSum{sh[w][v][2], sh[w][v][3]});
+    }
+    dot.mu[v] = make_double2(__dadd_rn(rr.s, rr.c), __dadd_rn(ii.s, ii.c));
+  }
+  if (threadIdx.x == 0)
+    *dot.counter = 0u;  // ready for the next launch on this stream
+}
+
+// ------------------------------------------------------------------ the operator row
+// acc += sum_m H_im x_{j_m} for one (site i, vector v), neighbours in ELL order.
+// Z > 0: the row length bound is known at compile time and the loop is unrolled.
+template <int V, int Z, class A, typename VT2>
+__device__ __forceinline__ void hop_row(const Op& op, int i, int v, const VT2* __restrict__ x,
+                                        double& tr, double& ti)
+{
+  const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+  if constexpr (Z > 0) {
+#pragma unroll
+    for (int m = 0; m < Z; ++m) {
+      if (m < cnt) {
+        const size_t e = (size_t)m * op.n + i;
+        const int j = op.nl[e];
+        const double2 h = op.hop[e];
+        const double2 y = ld(x + (size_t)j * V + v);
+        tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
+        ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
+      }
+    }
+  } else {
+    for (int m = 0; m < cnt; ++m) {
+      const size_t e = (size_t)m * op.n + i;
+      const int j = op.nl[e];
+      const double2 h = op.hop[e];
+      const double2 y = ld(x + (size_t)j * V + v);
+      tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
+      ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
+    }
+  }
+}
+
+enum StepMode { kApply = 0, kCheb = 1 };
+
+// out = H t1 / E_max (kApply) or out = 2 H t1 / E_max - t0 (kCheb), optionally fused
+// with the moment <left|out>. out may alias t0 (a site reads t0 before writing out).
+// Follows gpu_apply_hamiltonian / gpu_kernel_polynomial (src/hamiltonian.cu:153-186,
+// :886-925) with gpu_find_inner_product_1/2 (src/vector.cu:243-401) fused in.
+template <typename VT2, int V, int Z, class A, int MODE, bool DOT>
+__global__ void __launch_bounds__(kBlock) k_step(Op op, const VT2* t0,
+                                                 const VT2* __restrict__ t1, VT2* out,
+                                                 const VT2* __restrict__ left, Dot dot)
+{
+  const size_t total = (size_t)op.n * V;
+  CSum re{0.0, 0.0}, im{0.0, 0.0};
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / V);
+    const int v = (int)(g % V);
+    const double p = op.pot[i];
+    const double2 x = ld(t1 + g);
+    double tr = A::mul(p, x.x);
+    double ti = A::mul(p, x.y);
+    hop_row<V, Z, A>(op, i, v, t1, tr, ti);
+    tr = A::scale(tr, op);
+    ti = A::scale(ti, op);
+    if constexpr (MODE == kCheb) {
+      const double2 y0 = ld(t0 + g);
+      tr = A::two_x_minus(tr, y0.x);
+      ti = A::two_x_minus(ti, y0.y);
+    }
+    const double2 r = make_double2(tr, ti);
+    st(out + g, r);
+    if constexpr (DOT)
+      dot_term(re, im, stored(out, r), ld(left + g));
+  }
+  if constexpr (DOT)
+    dot_finish<V>(re, im, dot);
+}
+
+// <left|state> alone (moment 0).
+template <typename VT2, int V>
+__global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restrict__ state,
+                                                const VT2* __restrict__ left, Dot dot)
+{
+  CSum re{0.0, 0.0}, im{0.0, 0.0};
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock)
+    dot_term(re, im, ld(state + g), ld(left + g));
+  dot_finish<V>(re, im, dot);
+}
+
+// [X,H] in / E_max (src/hamiltonian.cu:240-271) or V in = -i sum H xx in
+// (src/hamiltonian.cu:323-352).
+template <typename VT2, int V, int Z, class A, bool CURRENT>
+__global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ in,
+                                                VT2* __restrict__ out)
+{
+  const size_t total = (size_t)op.n * V;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / V);
+    const int v = (int)(g % V);
+    const int cnt = op.uniform ? op.z : op.nn[i];
+    double tr = 0.0, ti = 0.0;
+    const int lim = Z > 0 ? Z : cnt;
+#pragma unroll
+    for (int m = 0; m < (Z > 0 ? Z : 1024); ++m) {
+      if (m >= lim || m >= cnt)
+        break;
+      const size_t e = (size_t)m * op.n + i;
+      const int j = op.nl[e];
+      const double2 h = op.hop[e];
+      const double2 y = ld(in + (size_t)j * V + v);
+      const double x = op.xx[e];
+      if constexpr (CURRENT) {
+        tr = A::add(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
+        ti = A::add(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
+      } else {
+        tr = A::sub(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
+        ti = A::sub(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
+      }
+    }
+    if constexpr (CURRENT) {
+      st(out + g, make_double2(ti, -tr));
+    } else {
+      st(out + g, make_double2(A::scale(tr, op), A::scale(ti, op)));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ time evolution
+// out accumulates in OT2 (the state itself in the FP64 form, an FP64 accumulator in
+// the FP32 form); the Chebyshev vectors are VT2.
+
+// gpu_chebyshev_01 (src/hamiltonian.cu:404-423); b1 already multiplied by direction.
+template <typename VT2, typename OT2, class A>
+__global__ void __launch_bounds__(kBlock) k_cheb01(size_t total, const VT2* __restrict__ s0,
+                                                   const VT2* __restrict__ s1, OT2* out,
+                                                   double b0, double b1)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const double2 a = ld(s0 + g), b = ld(s1 + g);
+    st(out + g, make_double2(A::add(A::mul(b0, a.x), A::mul(b1, b.y)),
+                             A::sub(A::mul(b0, a.y), A::mul(b1, b.x))));
+  }
+}
+
+// gpu_chebyshev_1x (src/hamiltonian.cu:619-633).
+template <typename VT2, typename OT2, class A>
+__global__ void __launch_bounds__(kBlock) k_cheb1x(size_t total, const VT2* __restrict__ s1x,
+                                                   OT2* out, double b1)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const double2 a = ld(s1x + g);
+    st(out + g, make_double2(A::mul(b1, a.y), A::mul(-b1, a.x)));
+  }
+}
+
+// The four accumulation labels of src/hamiltonian.cu:498-523 / :727-752.
+template <class A>
+__device__ __forceinline__ double2 accumulate(double2 o, double b, double tr, double ti,
+                                              int label)
+{
+  switch (label) {
+    case 1:
+      return make_double2(A::add(o.x, A::mul(b, tr)), A::add(o.y, A::mul(b, ti)));
+    case 2:
+      return make_double2(A::sub(o.x, A::mul(b, tr)), A::sub(o.y, A::mul(b, ti)));
+    case 3:
+      return make_double2(A::add(o.x, A::mul(b, ti)), A::sub(o.y, A::mul(b, tr)));
+    default:
+      return make_double2(A::sub(o.x, A::mul(b, ti)), A::add(o.y, A::mul(b, tr)));
+  }
+}
+
+// gpu_chebyshev_2 (src/hamiltonian.cu:465-529): s2 = 2 H s1 / E_max - s0 and
+// out += (label) * bessel * s2. s2 may alias s0.
+template <typename VT2, typename OT2, int V, int Z, class A>
+__global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
+                                                  const VT2* __restrict__ s1, VT2* s2,
+                                                  OT2* __restrict__ out, double bessel,
+                                                  int label)
+{
+  const size_t total = (size_t)op.n * V;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / V);
+    const int v = (int)(g % V);
+    const double p = op.pot[i];
+    const double2 x = ld(s1 + g);
+    double tr = A::mul(p, x.x), ti = A::mul(p, x.y);
+    hop_row<V, Z, A>(op, i, v, s1, tr, ti);
+    tr = A::scale(tr, op);
+    ti = A::scale(ti, op);
+    const double2 y0 = ld(s0 + g);
+    tr = A::two_x_minus(tr, y0.x);
+    ti = A::two_x_minus(ti, y0.y);
+    st(out + g, accumulate<A>(ld(out + g), bessel, tr, ti, label));
+    st(s2 + g, make_double2(tr, ti));
+  }
+}
+
+// gpu_chebyshev_2x (src/hamiltonian.cu:666-758): the coupled recurrences of T_m and
+// [X, T_m], accumulating out += (label) * bessel * [X, T_m]. s2 may alias s0 and s2x
+// may alias s0x.
+template <typename VT2, typename OT2, int V, int Z, class A>
+__global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const VT2* s0x,
+                                                   const VT2* __restrict__ s1,
+                                                   const VT2* __restrict__ s1x, VT2* s2,
+                                                   VT2* s2x, OT2* __restrict__ out,
+                                                   double bessel, int label)
+{
+  const size_t total = (size_t)op.n * V;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / V);
+    const int v = (int)(g % V);
+    const double p = op.pot[i];
+    const double2 a1 = ld(s1 + g), a1x = ld(s1x + g);
+    double tr = A::mul(p, a1.x), ti = A::mul(p, a1.y);
+    double txr = A::mul(p, a1x.x), txi = A::mul(p, a1x.y);
+    const int cnt = op.uniform ? op.z : op.nn[i];
+#pragma unroll
+    for (int m = 0; m < (Z > 0 ? Z : 1024); ++m) {
+      if (m >= cnt)
+        break;
+      const size_t e = (size_t)m * op.n + i;
+      const int j = op.nl[e];
+      const double2 h = op.hop[e];
+      const double2 c = ld(s1 + (size_t)j * V + v);
+      const double2 cx = ld(s1x + (size_t)j * V + v);
+      const double hre = A::cre(h.x, h.y, c.x, c.y);
+      const double him = A::cim(h.x, h.y, c.x, c.y);
+      tr = A::add(tr, hre);
+      ti = A::add(ti, him);
+      txr = A::add(txr, A::cre(h.x, h.y, cx.x, cx.y));
+      txi = A::add(txi, A::cim(h.x, h.y, cx.x, cx.y));
+      const double x = op.xx[e];
+      txr = A::sub(txr, A::mul(hre, x));
+      txi = A::sub(txi, A::mul(him, x));
+    }
+    const double2 y0 = ld(s0 + g), y0x = ld(s0x + g);
+    tr = A::two_x_minus(A::scale(tr, op), y0.x);
+    ti = A::two_x_minus(A::scale(ti, op), y0.y);
+    txr = A::two_x_minus(A::scale(txr, op), y0x.x);
+    txi = A::two_x_minus(A::scale(txi, op), y0x.y);
+    st(s2 + g, make_double2(tr, ti));
+    st(s2x + g, make_double2(txr, txi));
+    st(out + g, accumulate<A>(ld(out + g), bessel, txr, txi, label));
+  }
+}
+
+// ------------------------------------------------------------------ vector kernels
+template <typename VT2>
+__global__ void __launch_bounds__(kBlock) k_add(size_t total, VT2* __restrict__ dst,
+                                                const VT2* __restrict__ src)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const double2 a = ld(dst + g), b = ld(src + g);
+    st(dst + g, make_double2(__dadd_rn(a.x, b.x), __dadd_rn(a.y, b.y)));
+  }
+}
+
+// gpu_apply_sz (src/vector.cu:160-172): even sites copied, odd sites negated.
+template <typename VT2>
+__global__ void __launch_bounds__(kBlock) k_apply_sz(size_t total, int nvec,
+                                                     VT2* __restrict__ dst,
+                                                     const VT2* __restrict__ src)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const size_t i = g / (size_t)nvec;
+    VT2 a = src[g];
+    if (i & 1) {
+      a.x = -a.x;
+      a.y = -a.y;
+    }
+    dst[g] = a;
+  }
+}
+
+// Host split arrays (vector-major) <-> device interleaved [site][vector].
+template <typename VT2>
+__global__ void __launch_bounds__(kBlock) k_interleave(int n, int nvec,
+                                                       const double* __restrict__ re,
+                                                       const double* __restrict__ im,
+                                                       VT2* __restrict__ out)
+{
+  const size_t total = (size_t)n * nvec;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const size_t i = g / (size_t)nvec, k = g % (size_t)nvec;
+    st(out + g, make_double2(re[k * n + i], im[k * n + i]));
+  }
+}
+
+template <typename VT2>
+__global__ void __launch_bounds__(kBlock) k_deinterleave(int n, int nvec,
+                                                         const VT2* __restrict__ in,
+                                                         double* __restrict__ re,
+                                                         double* __restrict__ im)
+{
+  const size_t total = (size_t)n * nvec;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock) {
+    const size_t i = g / (size_t)nvec, k = g % (size_t)nvec;
+    const double2 a = ld(in + g);
+    re[k * n + i] = a.x;
+    im[k * n + i] = a.y;
+  }
+}
+
+// out[m] = sum_k in[m*segment + k], one block per segment (gpu_find_inner_product_2,
+// src/vector.cu:347-401), compensated.
+template <int UNUSED = 0>
+__global__ void __launch_bounds__(kBlock) k_segment_sum(const double2* __restrict__ in,
+                                                        int segment, double2* __restrict__ out)
+{
+  CSum re{0.0, 0.0}, im{0.0, 0.0};
+  const double2* base = in + (size_t)blockIdx.x * segment;
+  for (int k = threadIdx.x; k < segment; k += kBlock) {
+    csum_add(re, base[k].x);
+    csum_add(im, base[k].y);
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    csum_merge(re, shfl_xor(re, off));
+    csum_merge(im, shfl_xor(im, off));
+  }
+  __shared__ double sh[kBlock / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[warp][0] = re.s;
+    sh[warp][1] = re.c;
+    sh[warp][2] = im.s;
+    sh[warp][3] = im.c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CSum r{sh[0][0], sh[0][1]}, i{sh[0][2], sh[0][3]};
+    for (int w = 1; w < kBlock / 32; ++w) {
+      csum_merge(r, CSum{sh[w][0], sh[w][1]});
+      csum_merge(i, CSum{sh[w][2], sh[w][3]});
+    }
+    out[blockIdx.x] = make_double2(__dadd_rn(r.s, r.c), __dadd_rn(i.s, i.c));
+  }
+}
+
+// FP64 accumulator -> FP32 state (end of an FP32-form evolution).
+template <typename OT2>
+__global__ void __launch_bounds__(kBlock) k_narrow(size_t total, const double2* __restrict__ in,
+                                                   OT2* __restrict__ out)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock)
+    st(out + g, in[g]);
+}
+
+}  // namespace gqt

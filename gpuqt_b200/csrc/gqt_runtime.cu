@@ -1,0 +1,434 @@
+// Runtime part of the C ABI: errors, streams, device properties, vector and
+// Hamiltonian handles. See include/gpuqt.h for the contract of each entry point.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
+#include "gqt_algo.h"
+#include "gqt_forms.h"
+#include "gqt_internal.h"
+
+namespace gqt {
+
+namespace {
+thread_local std::string t_error;
+thread_local cudaStream_t t_stream = nullptr;
+thread_local uint64_t t_launches = 0;
+}  // namespace
+
+gqt_status fail(gqt_status code, const char* fmt, ...)
+{
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  std::vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  t_error = buf;
+  return code;
+}
+
+gqt_status cuda_fail(cudaError_t e, const char* what, const char* file, int line)
+{
+  return fail(e == cudaErrorMemoryAllocation ? GQT_ERR_ALLOC : GQT_ERR_CUDA,
+              "CUDA error %d (%s) in %s at %s:%d", (int)e, cudaGetErrorString(e), what, file,
+              line);
+}
+
+cudaStream_t stream() { return t_stream; }
+
+void count_launches(uint64_t k) { t_launches += k; }
+
+const DeviceInfo& device_info()
+{
+  static std::mutex mu;
+  static std::unordered_map<int, DeviceInfo> cache;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find(dev);
+  if (it == cache.end()) {
+    DeviceInfo info;
+    cudaDeviceGetAttribute(&info.sms, cudaDevAttrMultiProcessorCount, dev);
+    if (info.sms <= 0)
+      info.sms = 1;
+    it = cache.emplace(dev, info).first;
+  }
+  return it->second;
+}
+
+int max_grid() { return device_info().sms * (2048 / kBlock); }
+
+int grid_for(const void* kernel, size_t total)
+{
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> per_sm;
+  int bps;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = per_sm.find(kernel);
+    if (it == per_sm.end()) {
+      int b = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kBlock, 0) != cudaSuccess ||
+          b <= 0)
+        b = 1;
+      it = per_sm.emplace(kernel, b).first;
+    }
+    bps = it->second;
+  }
+  const size_t need = (total + kBlock - 1) / kBlock;
+  const size_t cap = (size_t)device_info().sms * bps;
+  size_t g = need < cap ? need : cap;
+  if (g < 1)
+    g = 1;
+  const int mg = max_grid();
+  return (int)(g < (size_t)mg ? g : (size_t)mg);
+}
+
+}  // namespace gqt
+
+using namespace gqt;
+
+namespace gqt_host {
+void set_error(const std::string& message) { gqt::fail(GQT_ERR_INPUT, "%s", message.c_str()); }
+}  // namespace gqt_host
+
+// ------------------------------------------------------------------ runtime
+extern "C" const char* gqt_last_error(void) { return t_error.c_str(); }
+
+extern "C" gqt_status gqt_version(int* major, int* minor)
+{
+  if (major)
+    *major = 1;
+  if (minor)
+    *minor = 0;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_set_stream(void* s)
+{
+  t_stream = (cudaStream_t)s;
+  return GQT_OK;
+}
+
+extern "C" void* gqt_get_stream(void) { return (void*)t_stream; }
+
+extern "C" gqt_status gqt_sync(void)
+{
+  GQT_CUDA(cudaStreamSynchronize(t_stream));
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+extern "C" uint64_t gqt_launch_count(void) { return t_launches; }
+extern "C" void gqt_reset_launch_count(void) { t_launches = 0; }
+
+// ------------------------------------------------------------------ vectors
+namespace {
+gqt_status check_vec(const gqt_vec* v, const char* what)
+{
+  if (!v || !v->data)
+    return fail(GQT_ERR_ARG, "%s: null vector", what);
+  return GQT_OK;
+}
+
+gqt_status same_shape(const gqt_vec* a, const gqt_vec* b, const char* what)
+{
+  GQT_TRY(check_vec(a, what));
+  GQT_TRY(check_vec(b, what));
+  if (a->n != b->n || a->nvec != b->nvec || a->precision != b->precision)
+    return fail(GQT_ERR_ARG, "%s: vectors differ in size, count or precision", what);
+  return GQT_OK;
+}
+
+const FormOps* ops_of(const gqt_vec* v, const char* what)
+{
+  const FormOps* f = form_ops(v->precision, v->nvec);
+  if (!f)
+    fail(GQT_ERR_ARG, "%s: unsupported vector form (precision %d, %d vectors)", what,
+         v->precision, v->nvec);
+  return f;
+}
+}  // namespace
+
+extern "C" gqt_status gqt_vec_create(int n, int nvec, int precision, gqt_vec** out)
+{
+  if (!out)
+    return fail(GQT_ERR_ARG, "gqt_vec_create: null output");
+  *out = nullptr;
+  if (n <= 0)
+    return fail(GQT_ERR_ARG, "gqt_vec_create: number of sites must be > 0 (got %d)", n);
+  if (!form_ops(precision, nvec))
+    return fail(GQT_ERR_ARG, "gqt_vec_create: unsupported form (precision %d, %d vectors)",
+                precision, nvec);
+  const size_t elem = precision == GQT_FP64 ? sizeof(double2) : sizeof(float2);
+  const size_t bytes = (size_t)n * (size_t)nvec * elem;
+  auto v = new (std::nothrow) gqt_vec;
+  if (!v)
+    return fail(GQT_ERR_ALLOC, "gqt_vec_create: host allocation failed");
+  v->n = n;
+  v->nvec = nvec;
+  v->precision = precision;
+  v->bytes = bytes;
+  cudaGetDevice(&v->device);
+  cudaError_t e = cudaMalloc(&v->data, bytes);
+  if (e != cudaSuccess) {
+    delete v;
+    return cuda_fail(e, "cudaMalloc(vector)", __FILE__, __LINE__);
+  }
+  e = cudaMemsetAsync(v->data, 0, bytes, t_stream);
+  if (e != cudaSuccess) {
+    cudaFree(v->data);
+    delete v;
+    return cuda_fail(e, "cudaMemsetAsync(vector)", __FILE__, __LINE__);
+  }
+  *out = v;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_clone(const gqt_vec* src, gqt_vec** out)
+{
+  GQT_TRY(check_vec(src, "gqt_vec_clone"));
+  GQT_TRY(gqt_vec_create(src->n, src->nvec, src->precision, out));
+  GQT_CUDA(cudaMemcpyAsync((*out)->data, src->data, src->bytes, cudaMemcpyDeviceToDevice,
+                           t_stream));
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_destroy(gqt_vec* v)
+{
+  if (!v)
+    return GQT_OK;
+  cudaError_t e = cudaSuccess;
+  if (v->data) {
+    // Pending work on the current stream may still read the buffer.
+    cudaStreamSynchronize(t_stream);
+    e = cudaFree(v->data);
+  }
+  delete v;
+  if (e != cudaSuccess)
+    return cuda_fail(e, "cudaFree(vector)", __FILE__, __LINE__);
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_info(const gqt_vec* v, int* n, int* nvec, int* precision)
+{
+  GQT_TRY(check_vec(v, "gqt_vec_info"));
+  if (n)
+    *n = v->n;
+  if (nvec)
+    *nvec = v->nvec;
+  if (precision)
+    *precision = v->precision;
+  return GQT_OK;
+}
+
+extern "C" void* gqt_vec_data(gqt_vec* v) { return v ? v->data : nullptr; }
+
+extern "C" gqt_status gqt_vec_upload(gqt_vec* v, const double* re, const double* im)
+{
+  GQT_TRY(check_vec(v, "gqt_vec_upload"));
+  if (!re || !im)
+    return fail(GQT_ERR_ARG, "gqt_vec_upload: null host array");
+  const FormOps* f = ops_of(v, "gqt_vec_upload");
+  if (!f)
+    return GQT_ERR_ARG;
+  const size_t count = (size_t)v->n * v->nvec;
+  double* stage = nullptr;
+  GQT_CUDA(cudaMallocAsync((void**)&stage, 2 * count * sizeof(double), t_stream));
+  gqt_status st = GQT_OK;
+  cudaError_t e = cudaMemcpyAsync(stage, re, count * sizeof(double), cudaMemcpyHostToDevice,
+                                  t_stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(stage + count, im, count * sizeof(double), cudaMemcpyHostToDevice,
+                        t_stream);
+  if (e != cudaSuccess)
+    st = cuda_fail(e, "cudaMemcpyAsync(upload)", __FILE__, __LINE__);
+  else
+    st = f->interleave(v->n, v->nvec, stage, stage + count, v->data);
+  cudaFreeAsync(stage, t_stream);
+  return st;
+}
+
+extern "C" gqt_status gqt_vec_download(const gqt_vec* v, double* re, double* im)
+{
+  GQT_TRY(check_vec(v, "gqt_vec_download"));
+  if (!re || !im)
+    return fail(GQT_ERR_ARG, "gqt_vec_download: null host array");
+  const FormOps* f = ops_of(v, "gqt_vec_download");
+  if (!f)
+    return GQT_ERR_ARG;
+  const size_t count = (size_t)v->n * v->nvec;
+  double* stage = nullptr;
+  GQT_CUDA(cudaMallocAsync((void**)&stage, 2 * count * sizeof(double), t_stream));
+  gqt_status st = f->deinterleave(v->n, v->nvec, v->data, stage, stage + count);
+  if (st == GQT_OK) {
+    cudaError_t e = cudaMemcpyAsync(re, stage, count * sizeof(double), cudaMemcpyDeviceToHost,
+                                    t_stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(im, stage + count, count * sizeof(double), cudaMemcpyDeviceToHost,
+                          t_stream);
+    if (e == cudaSuccess)
+      e = cudaStreamSynchronize(t_stream);
+    if (e != cudaSuccess)
+      st = cuda_fail(e, "download", __FILE__, __LINE__);
+  }
+  cudaFreeAsync(stage, t_stream);
+  return st;
+}
+
+extern "C" gqt_status gqt_vec_copy(gqt_vec* dst, const gqt_vec* src)
+{
+  GQT_TRY(same_shape(dst, src, "gqt_vec_copy"));
+  if (dst->data != src->data)
+    GQT_CUDA(cudaMemcpyAsync(dst->data, src->data, src->bytes, cudaMemcpyDeviceToDevice,
+                             t_stream));
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_add(gqt_vec* dst, const gqt_vec* src)
+{
+  GQT_TRY(same_shape(dst, src, "gqt_vec_add"));
+  return ops_of(dst, "gqt_vec_add")->add((size_t)dst->n * dst->nvec, dst->data, src->data);
+}
+
+extern "C" gqt_status gqt_vec_apply_sz(gqt_vec* dst, const gqt_vec* src)
+{
+  GQT_TRY(same_shape(dst, src, "gqt_vec_apply_sz"));
+  return ops_of(dst, "gqt_vec_apply_sz")
+    ->apply_sz((size_t)dst->n * dst->nvec, dst->nvec, dst->data, src->data);
+}
+
+extern "C" gqt_status gqt_vec_swap(gqt_vec* a, gqt_vec* b)
+{
+  GQT_TRY(same_shape(a, b, "gqt_vec_swap"));
+  std::swap(a->data, b->data);
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_zero(gqt_vec* v)
+{
+  GQT_TRY(check_vec(v, "gqt_vec_zero"));
+  GQT_CUDA(cudaMemsetAsync(v->data, 0, v->bytes, t_stream));
+  return GQT_OK;
+}
+
+// ------------------------------------------------------------------ Hamiltonian
+gqt_ham::~gqt_ham()
+{
+  ws.reset();
+  cudaFree(nn);
+  cudaFree(nl);
+  cudaFree(hop);
+  cudaFree(xx);
+  cudaFree(pot);
+}
+
+extern "C" gqt_status gqt_ham_create(const gqt_ell_desc* d, gqt_ham** out)
+{
+  if (!d || !out)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: null argument");
+  *out = nullptr;
+  const int n = d->n, z = d->max_neighbor;
+  if (n <= 0)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: number of sites must be > 0 (got %d)", n);
+  if (z <= 0)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: max_neighbor must be > 0 (got %d)", z);
+  if (!(d->energy_max > 0.0))
+    return fail(GQT_ERR_ARG, "gqt_ham_create: energy_max must be > 0 (got %g)", d->energy_max);
+  if (!d->neighbor_number || !d->neighbor_list || !d->potential || !d->hopping_real ||
+      !d->hopping_imag)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: null ELL array");
+  const size_t pairs = (size_t)n * z;
+  if (pairs > (size_t)1 << 40)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: n * max_neighbor too large");
+
+  // Validate on the host before anything reaches the device, then transpose to the
+  // column-major [m*n + i] layout (the transpose of src/hamiltonian.cu:47-88).
+  int uniform = 1;
+  for (int i = 0; i < n; ++i) {
+    const int c = d->neighbor_number[i];
+    if (c < 0 || c > z)
+      return fail(GQT_ERR_INPUT, "gqt_ham_create: site %d has %d neighbours (max_neighbor %d)",
+                  i, c, z);
+    if (c != z)
+      uniform = 0;
+    for (int m = 0; m < c; ++m) {
+      const int j = d->neighbor_list[(size_t)i * z + m];
+      if (j < 0 || j >= n)
+        return fail(GQT_ERR_INPUT, "gqt_ham_create: site %d neighbour %d index %d out of [0, %d)",
+                    i, m, j, n);
+    }
+  }
+  std::vector<int> nl(pairs, 0);
+  std::vector<double2> hop(pairs, make_double2(0.0, 0.0));
+  std::vector<double> xx(pairs, 0.0);
+  for (int i = 0; i < n; ++i) {
+    const int c = d->neighbor_number[i];
+    for (int m = 0; m < c; ++m) {
+      const size_t src = (size_t)i * z + m, dst = (size_t)m * n + i;
+      nl[dst] = d->neighbor_list[src];
+      hop[dst] = make_double2(d->hopping_real[src], d->hopping_imag[src]);
+      if (d->xx)
+        xx[dst] = d->xx[src];
+    }
+    // Padding entries point at the site itself with zero hopping; they are never
+    // read (the row length bounds every loop) but keep gathers in bounds.
+    for (int m = c; m < z; ++m)
+      nl[(size_t)m * n + i] = i;
+  }
+
+  auto h = new (std::nothrow) gqt_ham;
+  if (!h)
+    return fail(GQT_ERR_ALLOC, "gqt_ham_create: host allocation failed");
+  std::unique_ptr<gqt_ham> guard(h);
+  h->n = n;
+  h->z = z;
+  h->energy_max = d->energy_max;
+  h->uniform = uniform;
+  h->has_xx = d->xx != nullptr;
+  cudaGetDevice(&h->device);
+  GQT_CUDA(cudaMalloc(&h->nl, pairs * sizeof(int)));
+  GQT_CUDA(cudaMalloc(&h->hop, pairs * sizeof(double2)));
+  GQT_CUDA(cudaMalloc(&h->xx, pairs * sizeof(double)));
+  GQT_CUDA(cudaMalloc(&h->pot, (size_t)n * sizeof(double)));
+  if (!uniform) {
+    GQT_CUDA(cudaMalloc(&h->nn, (size_t)n * sizeof(int)));
+    GQT_CUDA(cudaMemcpy(h->nn, d->neighbor_number, (size_t)n * sizeof(int),
+                        cudaMemcpyHostToDevice));
+  }
+  GQT_CUDA(cudaMemcpy(h->nl, nl.data(), pairs * sizeof(int), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->hop, hop.data(), pairs * sizeof(double2), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->xx, xx.data(), pairs * sizeof(double), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->pot, d->potential, (size_t)n * sizeof(double),
+                      cudaMemcpyHostToDevice));
+  h->ws.reset(new_workspace());
+  *out = guard.release();
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_destroy(gqt_ham* h)
+{
+  if (h) {
+    cudaStreamSynchronize(t_stream);
+    delete h;
+  }
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_info(const gqt_ham* h, int* n, int* z, int* uniform, double* emax)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_info: null handle");
+  if (n)
+    *n = h->n;
+  if (z)
+    *z = h->z;
+  if (uniform)
+    *uniform = h->uniform;
+  if (emax)
+    *emax = h->energy_max;
+  return GQT_OK;
+}

@@ -1,0 +1,214 @@
+/* gpuqt.h — the C ABI of the B200 linear-scaling quantum transport library.
+ *
+ * Plain C types only: pointers, sizes, doubles. Every call returns a gqt_status
+ * (0 = success) and never exits the process; gqt_last_error() gives the message of
+ * the last failure on the calling thread. The C++ surface in include/lsqt/ (Model,
+ * Hamiltonian, Vector, find_* — the reference's own names) is a thin layer over
+ * these calls and turns a failure into the reference's print-and-exit.
+ *
+ * Each entry point names the reference interface it replaces (paths relative to the
+ * reference checkout). Device work is issued on the calling thread's current stream
+ * (gqt_set_stream); calls that return host data synchronise that stream.
+ *
+ * Layout on the device (owned by the handles):
+ *   vectors      interleaved complex, [site][vector] (double2 or float2)
+ *   Hamiltonian  ELL column-major [m*n + i]: int32 neighbour index, double2 hopping,
+ *                double xx; double on-site potential [n]; int32 row length [n] only
+ *                when rows are ragged.
+ */
+#ifndef GPUQT_H
+#define GPUQT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int gqt_status;
+enum {
+  GQT_OK = 0,
+  GQT_ERR_ARG = 1,     /* invalid argument (null handle, size mismatch, bad label) */
+  GQT_ERR_CUDA = 2,    /* a CUDA runtime call failed */
+  GQT_ERR_ALLOC = 3,   /* device or host allocation failed */
+  GQT_ERR_INPUT = 4,   /* malformed input file or model parameters */
+  GQT_ERR_IO = 5,      /* a file could not be opened or written */
+  GQT_ERR_STATE = 6    /* call not valid in the handle's current state */
+};
+
+/* Arithmetic forms of a Hamiltonian/vector pair. */
+enum {
+  GQT_FP64 = 0, /* plain: FP64 vectors, FP64 operator, reference operation order */
+  GQT_FP32 = 1  /* precision: FP32 vectors, FP64 operator and FP64 compensated sums */
+};
+
+typedef struct gqt_ham gqt_ham;
+typedef struct gqt_vec gqt_vec;
+
+/* ---------------------------------------------------------------- runtime */
+const char* gqt_last_error(void);
+gqt_status gqt_version(int* major, int* minor);
+/* Stream (a cudaStream_t) used by subsequent calls from this thread; NULL = legacy
+ * default stream, as the reference uses (src/hamiltonian.cu:228). */
+gqt_status gqt_set_stream(void* stream);
+void* gqt_get_stream(void);
+/* Synchronise the current stream and report any asynchronous kernel error. */
+gqt_status gqt_sync(void);
+/* Kernel launches this thread has issued since the last reset (all of them are this
+ * library's own kernels). */
+uint64_t gqt_launch_count(void);
+void gqt_reset_launch_count(void);
+
+/* ---------------------------------------------------------------- Hamiltonian */
+/* The model's ELL arrays, row-major [i*max_neighbor + m] on the host, exactly as
+ * Model holds them (src/model.h:55-60). Entries past neighbor_number[i] are ignored.
+ * xx may be NULL when the commutator/current are never applied. */
+typedef struct {
+  int n;
+  int max_neighbor;
+  double energy_max;
+  const int* neighbor_number;
+  const int* neighbor_list;
+  const double* potential;
+  const double* hopping_real;
+  const double* hopping_imag;
+  const double* xx;
+} gqt_ell_desc;
+
+/* Replaces Hamiltonian::Hamiltonian(Model&) / initialize_gpu
+ * (src/hamiltonian.cu:124-131, :27-89): validates every neighbour index on the host
+ * (0 <= j < n, row length <= max_neighbor) before anything is uploaded. */
+gqt_status gqt_ham_create(const gqt_ell_desc* desc, gqt_ham** out);
+/* Replaces Hamiltonian::~Hamiltonian (src/hamiltonian.cu:133-150). */
+gqt_status gqt_ham_destroy(gqt_ham* h);
+gqt_status gqt_ham_info(const gqt_ham* h, int* n, int* max_neighbor, int* uniform_rows,
+                        double* energy_max);
+
+/* ---------------------------------------------------------------- vectors */
+/* Replaces Vector::Vector(int) (src/vector.cu:61-70): nvec vectors of n sites,
+ * zero-initialised. precision is GQT_FP64 or GQT_FP32. */
+gqt_status gqt_vec_create(int n, int nvec, int precision, gqt_vec** out);
+/* Replaces Vector::Vector(Vector&) (src/vector.cu:92-105): deep copy. */
+gqt_status gqt_vec_clone(const gqt_vec* src, gqt_vec** out);
+/* Replaces Vector::~Vector (src/vector.cu:107-116). */
+gqt_status gqt_vec_destroy(gqt_vec* v);
+gqt_status gqt_vec_info(const gqt_vec* v, int* n, int* nvec, int* precision);
+/* Device address of the interleaved data ([site][vector] complex). */
+void* gqt_vec_data(gqt_vec* v);
+/* Replaces Vector::copy_from_host (src/vector.cu:199-208): split real/imag host
+ * arrays of n*nvec doubles, vector-major (vector k occupies [k*n, (k+1)*n)). */
+gqt_status gqt_vec_upload(gqt_vec* v, const double* real_part, const double* imag_part);
+/* Replaces Vector::copy_to_host (src/vector.cu:210-219). */
+gqt_status gqt_vec_download(const gqt_vec* v, double* real_part, double* imag_part);
+/* Replaces Vector::copy (src/vector.cu:140-148): dst = src. */
+gqt_status gqt_vec_copy(gqt_vec* dst, const gqt_vec* src);
+/* Replaces Vector::add (src/vector.cu:129-137): dst += src. */
+gqt_status gqt_vec_add(gqt_vec* dst, const gqt_vec* src);
+/* Replaces Vector::apply_sz (src/vector.cu:175-183): dst = S_z src (sign flips on odd
+ * sites). */
+gqt_status gqt_vec_apply_sz(gqt_vec* dst, const gqt_vec* src);
+/* Replaces Vector::swap (src/vector.cu:221-228): exchanges the device buffers. */
+gqt_status gqt_vec_swap(gqt_vec* a, gqt_vec* b);
+gqt_status gqt_vec_zero(gqt_vec* v);
+
+/* ---------------------------------------------------------------- operators */
+/* Replaces Hamiltonian::apply (src/hamiltonian.cu:225-237): out = H in / E_max. */
+gqt_status gqt_apply(const gqt_ham* h, const gqt_vec* in, gqt_vec* out);
+/* Replaces Hamiltonian::apply_commutator (:308-320): out = [X,H] in / E_max. */
+gqt_status gqt_apply_commutator(const gqt_ham* h, const gqt_vec* in, gqt_vec* out);
+/* Replaces Hamiltonian::apply_current (:387-399): out = V in (unscaled). */
+gqt_status gqt_apply_current(const gqt_ham* h, const gqt_vec* in, gqt_vec* out);
+/* Replaces Hamiltonian::kernel_polynomial (:970-984): s2 = 2 H s1 / E_max - s0.
+ * s2 may alias s0 (each site reads its s0 value before writing s2). */
+gqt_status gqt_kernel_polynomial(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
+                                 gqt_vec* s2);
+/* Replaces Hamiltonian::chebyshev_01 (:447-460). */
+gqt_status gqt_chebyshev_01(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
+                            gqt_vec* out, double bessel_0, double bessel_1, int direction);
+/* Replaces Hamiltonian::chebyshev_2 (:599-614); label 1..4 as in the reference. */
+gqt_status gqt_chebyshev_2(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
+                           gqt_vec* s2, gqt_vec* out, double bessel_m, int label);
+/* Replaces Hamiltonian::chebyshev_1x (:652-662). */
+gqt_status gqt_chebyshev_1x(const gqt_ham* h, const gqt_vec* in, gqt_vec* out,
+                            double bessel_1);
+/* Replaces Hamiltonian::chebyshev_2x (:856-882). */
+gqt_status gqt_chebyshev_2x(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s0x,
+                            const gqt_vec* s1, const gqt_vec* s1x, gqt_vec* s2,
+                            gqt_vec* s2x, gqt_vec* out, double bessel_m, int label);
+
+/* ---------------------------------------------------------------- reductions */
+/* Replaces Vector::inner_product_1 + inner_product_2 (src/vector.cu:331-344,
+ * :425-436) for one moment: <left|state> per vector, FP64 compensated sums.
+ * re/im hold nvec values. */
+gqt_status gqt_inner_product(const gqt_vec* state, const gqt_vec* left, double* re,
+                             double* im);
+
+/* Stage 1 of the reference's two-stage reduction (Vector::inner_product_1,
+ * src/vector.cu:331-344): <left|state> (nvec = 1) written to element `index` of the
+ * FP64 vector `target` on the device, without synchronising. */
+gqt_status gqt_inner_product_into(const gqt_vec* state, const gqt_vec* left, gqt_vec* target,
+                                  int index);
+/* Stage 2 (Vector::inner_product_2, src/vector.cu:425-436): out[m] = sum of
+ * in[m*segment .. m*segment+segment-1] for m < count; FP64 vectors, nvec = 1. */
+gqt_status gqt_vec_segment_sum(const gqt_vec* in, int segment, int count, gqt_vec* out);
+
+/* ---------------------------------------------------------------- algorithms */
+/* Replaces find_moments_chebyshev (src/sigma.cu:33-61):
+ * mu_m = <left| T_m(H/E_max) |right>, m = 0..n_moments-1, for each of the nvec
+ * vectors. mu_re/mu_im are host arrays of nvec*n_moments doubles, vector-major.
+ * The Chebyshev step and the moment partial sums run in one fused kernel per
+ * moment; the n_moments launches are replayed from a CUDA graph. */
+gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                       int n_moments, double* mu_re, double* mu_im);
+/* As gqt_moments, but leaves the moments on the device (mu_dev: nvec*n_moments
+ * double2 (re, im), moment-major [m*nvec + k]) and does not synchronise. */
+gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                              int n_moments, void* mu_dev);
+/* Replaces evolve (src/sigma.cu:116-151): state <- U(direction * dt) state with
+ * dt_scaled = dt * E_max. The Bessel coefficients J_m(dt_scaled) come from the host
+ * libm (j0/j1/jn) and the series stops at the first m >= 2 with |J_m| < 1e-15, as
+ * the reference does. */
+gqt_status gqt_evolve(const gqt_ham* h, int direction, double dt_scaled, gqt_vec* state);
+/* Replaces evolvex (src/sigma.cu:157-200): state <- [X, U(dt)] state (direction +1)
+ * or [U(-dt), X] state (direction -1). */
+gqt_status gqt_evolvex(const gqt_ham* h, int direction, double dt_scaled, gqt_vec* state);
+
+/* Replaces apply_damping + perform_chebyshev_summation (src/sigma.cu:76-110): the
+ * Jackson-damped Chebyshev sum of the real parts of mu at each energy (host work).
+ * mu_re/mu_im are damped in place, as the reference does. */
+gqt_status gqt_chebyshev_summation(int n_moments, double* mu_re, double* mu_im,
+                                   int n_energy, const double* energy, double energy_max,
+                                   double volume, double* out);
+
+/* ---------------------------------------------------------------- model and driver */
+typedef struct gqt_model gqt_model;
+/* Replaces Model::Model(std::string) (src/model.cu:30-65): reads para.in and the
+ * lattice or general-model files of input_dir, builds the ELL arrays and draws the
+ * disorder on the reference's single std::mt19937 stream (seed 12345678, as the
+ * reference's DEBUG build; the optional para.in keywords `seed`, `disorder_seed` and
+ * `phase_seed` override it). Diagnostics go to stdout as the reference prints them
+ * when verbose is nonzero. */
+gqt_status gqt_model_load(const char* input_dir, int verbose, gqt_model** out);
+gqt_status gqt_model_destroy(gqt_model* m);
+/* The model's ELL arrays (host memory owned by the model, valid until destroy). */
+gqt_status gqt_model_ell(const gqt_model* m, gqt_ell_desc* desc);
+/* Scalar parameters: number_of_moments, number_of_energy_points,
+ * number_of_steps_correlation, number_of_random_vectors, and volume. */
+gqt_status gqt_model_params(const gqt_model* m, int* n_moments, int* n_energy, int* n_steps,
+                            int* n_random_vectors, double* volume);
+gqt_status gqt_model_energy(const gqt_model* m, double* energy);
+gqt_status gqt_model_time_step(const gqt_model* m, double* time_step);
+/* Replaces Model::initialize_state (src/model.cu:77-109): the next random-phase
+ * vector (orbital < 0) or the local-orbital vector sqrt(N) e_orbital, drawn on the
+ * model's generator; re/im are n host doubles. */
+gqt_status gqt_model_initial_state(gqt_model* m, int orbital, double* re, double* im);
+/* Replaces lsqt(std::string) (src/lsqt.cu:135-152): the full run for one input
+ * directory, appending dos.out / vac0.out / vac.out / msd.out / S.out / ldos.out
+ * with the reference's formats. precision selects the arithmetic form. */
+gqt_status gqt_lsqt(const char* input_dir, int precision, int verbose);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
