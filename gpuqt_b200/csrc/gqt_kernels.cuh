@@ -326,11 +326,7 @@ __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ i
     const int v = (int)(g % V);
     const int cnt = op.uniform ? op.z : op.nn[i];
     double tr = 0.0, ti = 0.0;
-    const int lim = Z > 0 ? Z : cnt;
-#pragma unroll
-    for (int m = 0; m < (Z > 0 ? Z : 1024); ++m) {
-      if (m >= lim || m >= cnt)
-        break;
+    auto body = [&](int m) {
       const size_t e = (size_t)m * op.n + i;
       const int j = op.nl[e];
       const double2 h = op.hop[e];
@@ -343,6 +339,15 @@ __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ i
         tr = A::sub(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
         ti = A::sub(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
       }
+    };
+    if constexpr (Z > 0) {
+#pragma unroll
+      for (int m = 0; m < Z; ++m)
+        if (m < cnt)
+          body(m);
+    } else {
+      for (int m = 0; m < cnt; ++m)
+        body(m);
     }
     if constexpr (CURRENT) {
       st(out + g, make_double2(ti, -tr));
@@ -446,10 +451,7 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
     double tr = A::mul(p, a1.x), ti = A::mul(p, a1.y);
     double txr = A::mul(p, a1x.x), txi = A::mul(p, a1x.y);
     const int cnt = op.uniform ? op.z : op.nn[i];
-#pragma unroll
-    for (int m = 0; m < (Z > 0 ? Z : 1024); ++m) {
-      if (m >= cnt)
-        break;
+    auto body = [&](int m) {
       const size_t e = (size_t)m * op.n + i;
       const int j = op.nl[e];
       const double2 h = op.hop[e];
@@ -464,6 +466,15 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
       const double x = op.xx[e];
       txr = A::sub(txr, A::mul(hre, x));
       txi = A::sub(txi, A::mul(him, x));
+    };
+    if constexpr (Z > 0) {
+#pragma unroll
+      for (int m = 0; m < Z; ++m)
+        if (m < cnt)
+          body(m);
+    } else {
+      for (int m = 0; m < cnt; ++m)
+        body(m);
     }
     const double2 y0 = ld(s0 + g), y0x = ld(s0x + g);
     tr = A::two_x_minus(A::scale(tr, op), y0.x);
