@@ -1,0 +1,67 @@
+"""A short, fixed run of the KPM moment loop for profilers (ncu) and quick timing.
+
+    python -m gpuqt_b200.profile_case --workload graphene2m --form fp64 --moments 20 --sets 2
+
+Builds the workload's lattice, then runs `sets` moment sets of `moments` moments in
+one arithmetic form: fp64 (plain, one vector), fp32v1, or fp32vV (V vectors per
+launch, FP32 storage). Prints one JSON line with the measured rate.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import tempfile
+
+import numpy as np
+
+from . import workloads as W
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="graphene2m", choices=sorted(W.CONFIGS))
+    ap.add_argument("--form", default="fp64")
+    ap.add_argument("--moments", type=int, default=20)
+    ap.add_argument("--sets", type=int, default=2)
+    args = ap.parse_args()
+
+    import torch
+
+    import gpuqt_b200 as g
+
+    mo = re.fullmatch(r"(fp64|fp32)(?:v(\d+))?", args.form)
+    if not mo:
+        raise SystemExit(f"unknown form {args.form}")
+    prec = g.FP64 if mo.group(1) == "fp64" else g.FP32
+    V = int(mo.group(2) or 1)
+    tmp = tempfile.mkdtemp(prefix="gqt_prof_")
+    try:
+        m = g.Model.load(W.config_dir(tmp, args.workload))
+        H = g.Hamiltonian(m)
+        vecs = [m.initial_state() for _ in range(V)]
+        X = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
+                               nvec=V, precision=prec)
+        mu = torch.empty(2 * args.moments * V, dtype=torch.float64, device="cuda")
+        stream = torch.cuda.current_stream()
+        g.set_stream(stream.cuda_stream)
+        g.moments_device(H, X, X, args.moments, mu.data_ptr())
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(args.sets):
+            g.moments_device(H, X, X, args.moments, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        s = a.elapsed_time(b) / 1e3
+        print(json.dumps({"workload": args.workload, "form": args.form, "sites": m.n,
+                          "moments": args.moments, "sets": args.sets,
+                          "site_moments_per_s": V * m.n * args.moments * args.sets / s}))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+if __name__ == "__main__":
+    main()
