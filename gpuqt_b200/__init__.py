@@ -102,6 +102,7 @@ _SIGS = {
     "gqt_model_time_step": (ctypes.c_int, [_vp, _dp]),
     "gqt_model_initial_state": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
     "gqt_lsqt": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "gqt_chebyshev_step_noalloc": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 
 _lib = None

@@ -208,6 +208,34 @@ gqt_status gqt_model_initial_state(gqt_model* m, int orbital, double* re, double
  * with the reference's formats. precision selects the arithmetic form. */
 gqt_status gqt_lsqt(const char* input_dir, int precision, int verbose);
 
+/* ---------------------------------------------------------------- no-allocation step */
+/* No counterpart in the reference. One fused Chebyshev step with its moment, the
+ * kernel that gqt_moments repeats, for callers that drive the recurrence themselves
+ * and cannot let the library allocate device memory: a host that has already handed
+ * all of HBM to its own pool (a lattice sized to fill the GPU, or a framework's
+ * caching allocator) gets no memory from cudaMalloc, and in a loop that is being
+ * timed or captured, cudaMalloc's implicit device-wide synchronisation is not
+ * allowed either. This call allocates nothing: the block partials and the arrival
+ * counter of the moment reduction live in a static device array of
+ * GQT_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
+ *
+ *   mode 0: out = H t1 / E_max           (t0 ignored; the first step)
+ *   mode 1: out = 2 H t1 / E_max - t0    (out may alias t0)
+ *   mu_dev: device array of nvec double2 receiving <left|out> (re, im)
+ *
+ * FP64 vectors only (the reference's arithmetic; out is bit-identical to
+ * gqt_apply / gqt_kernel_polynomial). The launch uses at most
+ * GQT_NOALLOC_SCRATCH_BYTES / (32 * nvec) blocks; a call whose reduction would need
+ * more scratch than that is rejected with GQT_ERR_ARG. The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) and must come before
+ * any stream capture on that device. All calls share the one array: calls whose
+ * kernels can overlap on the GPU (different streams or threads, without ordering
+ * between them) race on it and must not be issued. */
+#define GQT_NOALLOC_SCRATCH_BYTES (1u << 20)
+gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, const gqt_vec* t0,
+                                      const gqt_vec* t1, gqt_vec* out, const gqt_vec* left,
+                                      void* mu_dev);
+
 #ifdef __cplusplus
 }
 #endif
