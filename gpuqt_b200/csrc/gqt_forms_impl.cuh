@@ -33,8 +33,18 @@ gqt_status launch(K* kernel, size_t total, Args... args)
   return GQT_OK;
 }
 
+// Vectors a thread advances per step launch: 4 float2 (two 16-byte loads) or 2 double2.
+template <typename VT2, int V>
+constexpr int vectors_per_thread()
+{
+  constexpr int w = std::is_same<VT2, float2>::value ? 4 : 2;
+  return V < w ? V : w;
+}
+
 template <typename VT2, int V, class A>
 struct FormImpl {
+  static constexpr int W = vectors_per_thread<VT2, V>();
+
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)
   {
@@ -46,6 +56,18 @@ struct FormImpl {
     Dot d = dot ? *dot : Dot{nullptr, nullptr, nullptr};
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
+      if constexpr (W > 1) {
+        // several vectors per thread: one launch item per (site, W vectors)
+        const size_t items = (size_t)op.n * (V / W);
+        if (mode == kApply) {
+          if (dot)
+            return launch(k_step_vec<VT2, V, W, Z, A, kApply, true>, items, op, a0, a1, o, l, d);
+          return launch(k_step_vec<VT2, V, W, Z, A, kApply, false>, items, op, a0, a1, o, l, d);
+        }
+        if (dot)
+          return launch(k_step_vec<VT2, V, W, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
+        return launch(k_step_vec<VT2, V, W, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
+      }
       if (mode == kApply) {
         if (dot)
           return launch(k_step<VT2, V, Z, A, kApply, true>, total, op, a0, a1, o, l, d);

@@ -24,6 +24,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <type_traits>
 
 namespace gqt {
 
@@ -152,28 +153,37 @@ __device__ __forceinline__ CSum shfl_xor(const CSum& a, int off)
   return b;
 }
 
-// Combine the per-thread partials of vector v = lane % V across the block, then
-// across the grid (last block, fixed order), and write dot.mu[v]. Must be reached
-// by every thread of the block.
-template <int V>
-__device__ __forceinline__ void dot_finish(CSum re, CSum im, const Dot& dot)
+// Combine per-thread partials across the block, then across the grid (last block,
+// fixed order), and write dot.mu[v] for v < V. A thread holds the sums of W
+// consecutive vectors v0 .. v0+W-1, v0 = (lane % (V/W)) * W. Must be reached by every
+// thread of the block.
+template <int V, int W>
+__device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const Dot& dot)
 {
   static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two <= 32");
+  static_assert(W >= 1 && W <= V && V % W == 0, "W must divide V");
+  constexpr int kTps = V / W;  // threads sharing one site
   constexpr int kWarps = kBlock / 32;
   __shared__ double sh[kWarps][V][4];
   __shared__ unsigned is_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 
 #pragma unroll
-  for (int off = 16; off >= V; off >>= 1) {
-    csum_merge(re, shfl_xor(re, off));
-    csum_merge(im, shfl_xor(im, off));
+  for (int off = 16; off >= kTps; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      csum_merge(re[k], shfl_xor(re[k], off));
+      csum_merge(im[k], shfl_xor(im[k], off));
+    }
   }
-  if (lane < V) {
-    sh[warp][lane][0] = re.s;
-    sh[warp][lane][1] = re.c;
-    sh[warp][lane][2] = im.s;
-    sh[warp][lane][3] = im.c;
+  if (lane < kTps) {
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      sh[warp][lane * W + k][0] = re[k].s;
+      sh[warp][lane * W + k][1] = re[k].c;
+      sh[warp][lane * W + k][2] = im[k].s;
+      sh[warp][lane * W + k][3] = im[k].c;
+    }
   }
   __syncthreads();
   if (threadIdx.x < V) {
@@ -229,6 +239,61 @@ __device__ __forceinline__ void dot_finish(CSum re, CSum im, const Dot& dot)
   }
   if (threadIdx.x == 0)
     *dot.counter = 0u;  // ready for the next launch on this stream
+}
+
+template <int V>
+__device__ __forceinline__ void dot_finish(CSum re, CSum im, const Dot& dot)
+{
+  CSum r[1] = {re}, i[1] = {im};
+  dot_finish_w<V, 1>(r, i, dot);
+}
+
+// ------------------------------------------------------------------ packed access
+// W consecutive complex elements of one site, as wide loads: two float2 per float4,
+// one double2 each. Offsets are multiples of W elements, so the loads are aligned.
+template <int W>
+__device__ __forceinline__ void ldw(const float2* p, double2 (&o)[W])
+{
+  if constexpr (W == 1) {
+    o[0] = ld(p);
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k) {
+      const float4 f = reinterpret_cast<const float4*>(p)[k];
+      o[2 * k] = make_double2((double)f.x, (double)f.y);
+      o[2 * k + 1] = make_double2((double)f.z, (double)f.w);
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void ldw(const double2* p, double2 (&o)[W])
+{
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    o[k] = p[k];
+}
+
+template <int W>
+__device__ __forceinline__ void stw(float2* p, const double2 (&v)[W])
+{
+  if constexpr (W == 1) {
+    st(p, v[0]);
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k)
+      reinterpret_cast<float4*>(p)[k] =
+        make_float4(__double2float_rn(v[2 * k].x), __double2float_rn(v[2 * k].y),
+                    __double2float_rn(v[2 * k + 1].x), __double2float_rn(v[2 * k + 1].y));
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void stw(double2* p, const double2 (&v)[W])
+{
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    p[k] = v[k];
 }
 
 // ------------------------------------------------------------------ the operator row
@@ -311,6 +376,91 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
        g += (size_t)gridDim.x * kBlock)
     dot_term(re, im, ld(state + g), ld(left + g));
   dot_finish<V>(re, im, dot);
+}
+
+// Batched step: each thread advances W consecutive vectors of one site, so a site's
+// ELL row, potential and row length are read once per W vectors and every vector
+// access is a wide load. Same arithmetic per element as k_step; with FastArith the
+// moment uses the FP64 value of T_m before its FP32 rounding and plain FP64 per-thread
+// sums (a few dozen terms each), merged with TwoSum across lanes, blocks and the grid.
+template <typename VT2, int V, int W, int Z, class A, int MODE, bool DOT>
+__global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
+                                                     const VT2* __restrict__ t1, VT2* out,
+                                                     const VT2* __restrict__ left, Dot dot)
+{
+  constexpr int kTps = V / W;
+  constexpr bool kExact = std::is_same<A, ExactArith>::value;
+  const size_t items = (size_t)op.n * kTps;
+  CSum re[W], im[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    re[k] = im[k] = CSum{0.0, 0.0};
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < items;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / kTps);
+    const int v0 = (int)(g % kTps) * W;
+    const size_t base = (size_t)i * V + v0;
+    const double p = op.pot[i];
+    double2 x[W];
+    ldw<W>(t1 + base, x);
+    double tr[W], ti[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      tr[k] = A::mul(p, x[k].x);
+      ti[k] = A::mul(p, x[k].y);
+    }
+    const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+    auto body = [&](int m) {
+      const size_t e = (size_t)m * op.n + i;
+      const int j = op.nl[e];
+      const double2 h = op.hop[e];
+      double2 y[W];
+      ldw<W>(t1 + (size_t)j * V + v0, y);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+        ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+      }
+    };
+    if constexpr (Z > 0) {
+#pragma unroll
+      for (int m = 0; m < Z; ++m)
+        if (m < cnt)
+          body(m);
+    } else {
+      for (int m = 0; m < cnt; ++m)
+        body(m);
+    }
+    double2 r[W];
+    if constexpr (MODE == kCheb) {
+      double2 y0[W];
+      ldw<W>(t0 + base, y0);
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        r[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0[k].x),
+                            A::two_x_minus(A::scale(ti[k], op), y0[k].y));
+    } else {
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        r[k] = make_double2(A::scale(tr[k], op), A::scale(ti[k], op));
+    }
+    stw<W>(out + base, r);
+    if constexpr (DOT) {
+      double2 l[W];
+      ldw<W>(left + base, l);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        if constexpr (kExact) {
+          dot_term(re[k], im[k], stored(out, r[k]), l[k]);
+        } else {
+          re[k].s = fma(r[k].x, l[k].x, fma(r[k].y, l[k].y, re[k].s));
+          im[k].s = fma(r[k].y, l[k].x, fma(-r[k].x, l[k].y, im[k].s));
+        }
+      }
+    }
+  }
+  if constexpr (DOT)
+    dot_finish_w<V, W>(re, im, dot);
 }
 
 // [X,H] in / E_max (src/hamiltonian.cu:240-271) or V in = -i sum H xx in
