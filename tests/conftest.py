@@ -16,7 +16,7 @@ INPUTS = os.path.join(GOLDEN, "inputs")
 REF = os.path.join(GOLDEN, "ref")
 EXAMPLES = os.path.join(GOLDEN, "examples")
 SMALL_FIXTURES = ["sq16_pbc", "sq12_open_vac", "graphene_8x4", "cubic6", "chain_z2",
-                  "sq20_charge", "general40"]
+                  "sq20_charge", "general40", "general_spin"]
 ORACLE_FIXTURES = ["sq16_pbc", "sq12_open_vac", "graphene_8x4", "cubic6", "chain_z2"]
 
 

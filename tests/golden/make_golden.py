@@ -139,6 +139,11 @@ FIXTURES = {
     "general40": ("model 0\nenergy_max 9.0\nnumber_of_moments 150\ncalculate_msd\n"
                   "calculate_vac\n",
                   None, energies(-8.0, 8.0, 17), [0.4, 0.4], general_model_files(), 9.0),
+    "general_spin": ("model 0\nenergy_max 9.0\nnumber_of_moments 120\ncalculate_spin\n"
+                     "calculate_ldos\n",
+                     None, energies(-8.0, 8.0, 17), [0.5, 0.5, 0.5],
+                     dict(general_model_files(n=48, z=4, seed=77),
+                          **{"local_orbitals.in": "3\n0\n7\n21\n"}), 9.0),
     # The CPU-runnable plain FP64 case: 256 x 256 square lattice, t = -1, W = 2,
     # energy scale 5, 1000 moments, VAC with 10 steps of 1.0; disorder seed 1, phase
     # seed 7 (split-seed mode).
@@ -148,6 +153,7 @@ FIXTURES = {
                   energies(-4.95, 4.95, 199), [1.0] * 10, None, None),
 }
 SPLIT_SEEDS = {"square256": (1, 7)}
+OUT_FILES = ("dos.out", "vac0.out", "vac.out", "msd.out", "S.out", "ldos.out")
 
 
 def ref_para(para: str) -> str:
@@ -194,7 +200,7 @@ def main() -> None:
                                    for k, v in ops.items()})
         if seeds is None:
             # The reference's own .out files for the full run of this directory.
-            for f in ("dos.out", "vac0.out", "vac.out", "msd.out"):
+            for f in OUT_FILES:
                 p = os.path.join(rd, f)
                 if os.path.exists(p):
                     os.remove(p)
@@ -202,7 +208,7 @@ def main() -> None:
                 f.write(rd + "\n")
             subprocess.run([oracle.REF_LSQT, os.path.join(tmp, "input.txt")], check=True,
                            stdout=subprocess.DEVNULL)
-            for f in ("dos.out", "vac0.out", "vac.out", "msd.out"):
+            for f in OUT_FILES:
                 p = os.path.join(rd, f)
                 if os.path.exists(p):
                     shutil.copy(p, os.path.join(o, f))

@@ -51,7 +51,7 @@ def test_cli_matches_reference_outputs(tmp_path, name):
                        text=True)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     found = 0
-    for f in ("dos.out", "vac0.out", "vac.out", "msd.out"):
+    for f in ("dos.out", "vac0.out", "vac.out", "msd.out", "S.out", "ldos.out"):
         ref = os.path.join(REF, name, f)
         if os.path.exists(ref):
             _compare(str(d / f), ref)
