@@ -309,21 +309,32 @@ def run_ours(args):
             g.moments(H, x, x, M)
         barrier(world)
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
+        marks = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
+        wall0 = time.perf_counter()
+        marks[0].record(stream)
+        for k in range(args.steps):
             x.upload_ptr(re_h.data_ptr(), im_h.data_ptr())
+            marks[2 * k + 1].record(stream)
             mr, mi = g.moments(H, x, x, M)
-        e1.record(stream)
+            marks[2 * k + 2].record(stream)
         torch.cuda.synchronize()
-        e_ms = max_over_ranks(e0.elapsed_time(e1), world)
+        wall = time.perf_counter() - wall0
+        e_ms = max_over_ranks(marks[0].elapsed_time(marks[-1]), world)
+        up = sum(marks[2 * k].elapsed_time(marks[2 * k + 1]) for k in range(args.steps))
+        mo = sum(marks[2 * k + 1].elapsed_time(marks[2 * k + 2]) for k in range(args.steps))
         e2e = {"value": world * n * M * args.steps / (e_ms / 1e3), "unit": UNIT,
-               "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": M * 16}
+               "h2d_bytes_per_step": 2 * n * 8, "d2h_bytes_per_step": M * 16,
+               "ms_upload_per_step": up / args.steps, "ms_moments_per_step": mo / args.steps,
+               "wall_ms_per_step": wall * 1e3 / args.steps}
 
         forms = None
         evolution = None
         if not args.no_forms:
             forms, evolution = measure_forms(g, torch, m, H, phi, args, stream, hbm_peak)
+        batch = None
+        if not args.no_batch:
+            del x
+            batch = measure_batch(g, torch, tmp, stream, hbm_peak)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_line(reference_dir(src, os.path.join(tmp, "ref")), n)
@@ -351,6 +362,7 @@ def run_ours(args):
                 "clocks": clocks,
                 "forms": forms,
                 "evolution": evolution,
+                "batch": batch,
             }
             print(json.dumps(line), flush=True)
     finally:
@@ -428,6 +440,63 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
     return out, evolution
 
 
+def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
+    """The realisation batch: 8 uneven square lattices in one block-diagonal operator,
+    `vectors` random-phase vectors each, FP32 storage, vectors per launch chosen by the
+    autotuner; one moment set per vector block. Reports the rate over the whole job and
+    the DOS error of one vector against its FP64 moments."""
+    from gpuqt_b200 import workloads as W
+    dirs = W.batch_dirs(os.path.join(tmp, "batch"), moments=moments)
+    models = [g.Model.load(d) for d in dirs]
+    B = g.Hamiltonian.batch(models)
+    best, rates = g.autotune_nvec(B, g.FP32, 20, [4, 8, 16, 32])
+    V = best
+    rng = np.random.default_rng(11)
+    sites = sum(m.n for m in models)
+    X = g.Vector(B.n, nvec=V, precision=g.FP32)
+    mu = torch.empty(2 * moments * len(models) * V, dtype=torch.float64, device="cuda")
+
+    def fill():
+        per = []
+        for m in models:
+            ph = rng.uniform(0.0, 2 * np.pi, size=(V, m.n))
+            per.append((np.cos(ph), np.sin(ph)))
+        X.upload(*B.scatter(per))
+        return per
+
+    per0 = fill()
+    g.moments_device(B, X, X, moments, mu.data_ptr())  # warm-up, graph capture
+    torch.cuda.synchronize()
+    blocks = vectors // V
+    total_ms = 0.0
+    for k in range(blocks):
+        if k:
+            fill()  # host generation and upload stay outside the timed kernels
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.moments_device(B, X, X, moments, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        total_ms += a.elapsed_time(b)
+    rate = vectors * sites * moments / (total_ms / 1e3)
+    bytes_site_moment = fp32_bytes_per_site_vector(V, z=4) * B.n / sites
+    # DOS error of vector 0 of realisation 0 against its FP64 moments
+    X.upload(*B.scatter(per0))
+    r32, i32 = g.moments(B, X, X, moments)
+    m0 = models[0]
+    H0 = g.Hamiltonian(m0)
+    x0 = g.Vector.from_host(per0[0][0][0], per0[0][1][0])
+    r64, i64 = g.moments(H0, x0, x0, moments)
+    err = dos_error(g, m0, (r64, i64), (r32[0, 0], i32[0, 0]))
+    return {"realisations": [[m.n, round(m.energy_max, 4)] for m in models],
+            "sites": sites, "padded_sites": B.n, "vectors": vectors, "moments": moments,
+            "autotuned_vectors_per_launch": V, "autotune_rates": rates,
+            "site_moments_per_s": rate, "ms_total": total_ms,
+            "achieved_gbs": rate * bytes_site_moment / 1e9,
+            "frac": rate * bytes_site_moment / 1e9 / hbm_peak,
+            "dos_err_vs_fp64": err}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -436,6 +505,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -63,6 +63,12 @@ _SIGS = {
     "gqt_ham_create": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.POINTER(_vp)]),
     "gqt_ham_destroy": (ctypes.c_int, [_vp]),
     "gqt_ham_info": (ctypes.c_int, [_vp, _ip, _ip, _ip, _dp]),
+    "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
+                                            ctypes.POINTER(_vp)]),
+    "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
+    "gqt_ham_realisation": (ctypes.c_int, [_vp, ctypes.c_int, _ip, _ip, _dp]),
+    "gqt_autotune_nvec": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _ip, ctypes.c_int, _ip,
+                                         _dp]),
     "gqt_vec_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                       ctypes.POINTER(_vp)]),
     "gqt_vec_clone": (ctypes.c_int, [_vp, ctypes.POINTER(_vp)]),
@@ -317,12 +323,69 @@ class Hamiltonian:
         d.xx = _dptr(self._keep["xx"]) if "xx" in self._keep else None
         h = _vp()
         _call("gqt_ham_create", ctypes.byref(d), ctypes.byref(h))
+        self._adopt(h)
+
+    def _adopt(self, h) -> None:
         self.h = h
         self._keep = None
-        self.n, self.max_neighbor, self.energy_max = n, z, float(arrays["energy_max"])
-        u = ctypes.c_int()
-        _call("gqt_ham_info", self.h, None, None, ctypes.byref(u), None)
+        n, z, u, e = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        _call("gqt_ham_info", self.h, ctypes.byref(n), ctypes.byref(z), ctypes.byref(u),
+              ctypes.byref(e))
+        self.n, self.max_neighbor, self.energy_max = n.value, z.value, e.value
         self.uniform_rows = bool(u.value)
+        r = ctypes.c_int()
+        _call("gqt_ham_realisations", self.h, ctypes.byref(r))
+        self.n_real = r.value
+        self.realisations = []
+        for k in range(self.n_real):
+            off, nr, em = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+            _call("gqt_ham_realisation", self.h, k, ctypes.byref(off), ctypes.byref(nr),
+                  ctypes.byref(em))
+            self.realisations.append((off.value, nr.value, em.value))
+
+    @classmethod
+    def batch(cls, models) -> "Hamiltonian":
+        """A realisation batch: independent models as one block-diagonal operator
+        (gqt_ham_create_batch); accepts Model objects or ELL dicts."""
+        descs = (EllDesc * len(models))()
+        keep = []
+        for k, mdl in enumerate(models):
+            a = mdl.ell() if hasattr(mdl, "ell") else mdl
+            arr = {
+                "nn": np.ascontiguousarray(a["neighbor_number"], dtype=np.int32),
+                "nl": np.ascontiguousarray(a["neighbor_list"], dtype=np.int32),
+                "pot": np.ascontiguousarray(a["potential"], dtype=np.float64),
+                "hr": np.ascontiguousarray(a["hopping_real"], dtype=np.float64),
+                "hi": np.ascontiguousarray(a["hopping_imag"], dtype=np.float64),
+            }
+            if a.get("xx") is not None:
+                arr["xx"] = np.ascontiguousarray(a["xx"], dtype=np.float64)
+            keep.append(arr)
+            d = descs[k]
+            d.n, d.max_neighbor = int(a["n"]), int(a["max_neighbor"])
+            d.energy_max = float(a["energy_max"])
+            d.neighbor_number = arr["nn"].ctypes.data_as(_ip)
+            d.neighbor_list = arr["nl"].ctypes.data_as(_ip)
+            d.potential = _dptr(arr["pot"])
+            d.hopping_real = _dptr(arr["hr"])
+            d.hopping_imag = _dptr(arr["hi"])
+            d.xx = _dptr(arr["xx"]) if "xx" in arr else None
+        h = _vp()
+        _call("gqt_ham_create_batch", descs, len(models), ctypes.byref(h))
+        obj = cls.__new__(cls)
+        obj._adopt(h)
+        return obj
+
+    def scatter(self, per_model: list) -> tuple[np.ndarray, np.ndarray]:
+        """Host arrays (nvec * n, vector-major) of a batch vector from per-model
+        (re, im) arrays of shape (nvec, n_r); padding sites are zero."""
+        nvec = np.atleast_2d(per_model[0][0]).shape[0]
+        re = np.zeros((nvec, self.n))
+        im = np.zeros((nvec, self.n))
+        for (off, nr, _), (r, i) in zip(self.realisations, per_model):
+            re[:, off:off + nr] = np.atleast_2d(r)
+            im[:, off:off + nr] = np.atleast_2d(i)
+        return re, im
 
     def close(self) -> None:
         if self.h is not None and _lib is not None:
@@ -377,13 +440,28 @@ def inner_product(state: Vector, left: Vector):
 
 
 def moments(H: Hamiltonian, left: Vector, right: Vector, n_moments: int):
-    """mu_m = <left|T_m(H/E_max)|right>; arrays of shape (n_moments,) or (nvec, n_moments)."""
-    re = np.zeros(n_moments * right.nvec)
-    im = np.zeros(n_moments * right.nvec)
+    """mu_m = <left|T_m(H/E_max)|right>: shape (n_moments,), (nvec, n_moments), or for a
+    realisation batch (n_real, nvec, n_moments)."""
+    R = getattr(H, "n_real", 1)
+    re = np.zeros(n_moments * right.nvec * R)
+    im = np.zeros(n_moments * right.nvec * R)
     _call("gqt_moments", H.h, left.h, right.h, n_moments, _dptr(re), _dptr(im))
+    if R > 1:
+        return re.reshape(R, right.nvec, n_moments), im.reshape(R, right.nvec, n_moments)
     if right.nvec > 1:
         return re.reshape(right.nvec, n_moments), im.reshape(right.nvec, n_moments)
     return re, im
+
+
+def autotune_nvec(H: Hamiltonian, precision: int, n_moments: int, candidates):
+    """The vectors-per-launch candidate with the highest measured site-moments/s
+    (gqt_autotune_nvec); returns (best, {candidate: rate})."""
+    c = np.ascontiguousarray(candidates, dtype=np.int32)
+    rates = np.zeros(c.size)
+    best = ctypes.c_int()
+    _call("gqt_autotune_nvec", H.h, precision, n_moments, c.ctypes.data_as(_ip), c.size,
+          ctypes.byref(best), _dptr(rates))
+    return best.value, dict(zip(c.tolist(), rates.tolist()))
 
 
 def moments_device(H: Hamiltonian, left: Vector, right: Vector, n_moments: int,

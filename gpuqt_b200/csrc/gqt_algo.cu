@@ -51,26 +51,35 @@ gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i
   return GQT_OK;
 }
 
-gqt_status ws_dot(Workspace& ws, int nvec, DotScratch** out)
+gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out)
 {
-  if (!ws.dot.partials) {
-    const int blocks = max_grid();
-    GQT_CUDA(cudaMalloc(&ws.dot.partials, (size_t)blocks * 32 * 4 * sizeof(double)));
+  const size_t need = doubles > (size_t)max_grid() * 32 * 4 ? doubles : (size_t)max_grid() * 32 * 4;
+  if ((size_t)ws.dot.blocks < need) {
+    cudaStreamSynchronize(stream());
+    // Graphs captured with the old buffer can never run again.
+    for (auto& kv : ws.graphs)
+      cudaGraphExecDestroy(kv.second);
+    ws.graphs.clear();
+    cudaFree(ws.dot.partials);
+    ws.dot.partials = nullptr;
+    ws.dot.blocks = 0;
+    GQT_CUDA(cudaMalloc(&ws.dot.partials, need * sizeof(double)));
+    ws.dot.blocks = (int)need;  // capacity in doubles
+  }
+  if (!ws.dot.counter) {
     GQT_CUDA(cudaMalloc(&ws.dot.counter, sizeof(unsigned)));
     GQT_CUDA(cudaMemset(ws.dot.counter, 0, sizeof(unsigned)));
-    ws.dot.blocks = blocks;
-    ws.dot.nvec = 32;
   }
-  (void)nvec;
   *out = &ws.dot;
   return GQT_OK;
 }
 
 namespace {
 
-Op make_op(const gqt_ham* h)
+Op make_op(const gqt_ham* h, int nvec = 1)
 {
   Op op;
+  op.wpt = (nvec >= 0 && nvec <= 32) ? h->wpt[nvec] : 0;
   op.n = h->n;
   op.z = h->z;
   op.uniform = h->uniform;
@@ -161,9 +170,29 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
                            const gqt_vec* right, int M, double2* mu, void* A, void* B,
                            DotScratch* ds)
 {
-  const Op op = make_op(h);
+  const Op op = make_op(h, right->nvec);
   const int V = right->nvec;
   const size_t total = (size_t)h->n * V;
+  if (h->n_real > 1) {
+    // Realisation batch: the same sequence with per-realisation moments.
+    const int RV = h->n_real * V;
+    MultiDot md{ds->partials, mu, h->tile_first, h->n_tiles, h->tile_sites, h->n_real, 0};
+    GQT_TRY(f->step_multi(op, kDotOnly, nullptr, right->data, nullptr, left->data, md));
+    if (M < 2)
+      return GQT_OK;
+    md.mu = mu + RV;
+    GQT_TRY(f->step_multi(op, kApply, nullptr, right->data, A, left->data, md));
+    const void* prev = right->data;
+    void* cur = A;
+    for (int m = 2; m < M; ++m) {
+      void* out = (prev == right->data) ? B : (void*)prev;
+      md.mu = mu + (size_t)m * RV;
+      GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, left->data, md));
+      prev = cur;
+      cur = out;
+    }
+    return GQT_OK;
+  }
   Dot d{ds->partials, ds->counter, mu};
   GQT_TRY(f->dot(total, right->data, left->data, d));
   if (M < 2)
@@ -198,7 +227,7 @@ extern "C" gqt_status gqt_apply(const gqt_ham* h, const gqt_vec* in, gqt_vec* ou
   const FormOps* f = ops_for(in, "gqt_apply");
   if (!f)
     return GQT_ERR_ARG;
-  return f->step(make_op(h), kApply, nullptr, in->data, out->data, nullptr, nullptr);
+  return f->step(make_op(h, in->nvec), kApply, nullptr, in->data, out->data, nullptr, nullptr);
 }
 
 static gqt_status xop_entry(const gqt_ham* h, const gqt_vec* in, gqt_vec* out, bool current,
@@ -210,6 +239,8 @@ static gqt_status xop_entry(const gqt_ham* h, const gqt_vec* in, gqt_vec* out, b
     return fail(GQT_ERR_ARG, "%s: input and output must differ", what);
   if (!h->has_xx)
     return fail(GQT_ERR_STATE, "%s: the Hamiltonian was created without xx", what);
+  if (h->n_real > 1)
+    return fail(GQT_ERR_STATE, "%s: not defined on a realisation batch", what);
   const FormOps* f = ops_for(in, what);
   if (!f)
     return GQT_ERR_ARG;
@@ -237,7 +268,7 @@ extern "C" gqt_status gqt_kernel_polynomial(const gqt_ham* h, const gqt_vec* s0,
   const FormOps* f = ops_for(s1, "gqt_kernel_polynomial");
   if (!f)
     return GQT_ERR_ARG;
-  return f->step(make_op(h), kCheb, s0->data, s1->data, s2->data, nullptr, nullptr);
+  return f->step(make_op(h, s1->nvec), kCheb, s0->data, s1->data, s2->data, nullptr, nullptr);
 }
 
 extern "C" gqt_status gqt_chebyshev_01(const gqt_ham* h, const gqt_vec* s0, const gqt_vec* s1,
@@ -417,7 +448,8 @@ static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const g
   const size_t bytes = right->bytes;
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
-  GQT_TRY(ws_dot(ws, right->nvec, ds));
+  // Block partials: [grid][R][V][4] doubles for a batch, [grid][V][4] otherwise.
+  GQT_TRY(ws_dot(ws, (size_t)max_grid() * h->n_real * right->nvec * 4, ds));
   return GQT_OK;
 }
 
@@ -495,7 +527,7 @@ extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const g
   if (M < 1)
     return fail(GQT_ERR_ARG, "gqt_moments: number of moments must be > 0 (got %d)", M);
   Workspace& ws = *h->ws;
-  const int V = right->nvec;
+  const int V = right->nvec * h->n_real;  // results per moment: [r][vector]
   const size_t need = (size_t)M * V * sizeof(double2);
   if (ws.mu_bytes < need) {
     cudaStreamSynchronize(stream());
@@ -531,6 +563,8 @@ static gqt_status evolve_common(const gqt_ham* h, int direction, double dt, gqt_
     return fail(GQT_ERR_ARG, "%s: direction must be +1 or -1 (got %d)", w, direction);
   if (commutator && !h->has_xx)
     return fail(GQT_ERR_STATE, "%s: the Hamiltonian was created without xx", w);
+  if (h->n_real > 1)
+    return fail(GQT_ERR_STATE, "%s: a realisation batch has one time scale per model", w);
   const FormOps* f = ops_for(state, w);
   if (!f)
     return GQT_ERR_ARG;
@@ -647,5 +681,106 @@ extern "C" gqt_status gqt_chebyshev_summation(int M, double* mu_re, double* mu_i
     temp /= std::sqrt(1.0 - es * es);
     out[e] = temp / energy_max;
   }
+  return GQT_OK;
+}
+
+// ------------------------------------------------------------------ autotuner
+extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_moments,
+                                        const int* candidates, int n_candidates, int* best,
+                                        double* rates)
+{
+  const char* w = "gqt_autotune_nvec";
+  if (!h || !candidates || n_candidates < 1 || !best)
+    return fail(GQT_ERR_ARG, "%s: null argument or no candidates", w);
+  if (n_moments < 2)
+    return fail(GQT_ERR_ARG, "%s: needs at least 2 probe moments", w);
+  long long sites = 0;
+  for (int r = 0; r < h->n_real; ++r)
+    sites += h->real_n[r];
+  cudaStream_t s = stream();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  GQT_CUDA(cudaEventCreate(&e0));
+  GQT_CUDA(cudaEventCreate(&e1));
+  double best_rate = -1.0;
+  gqt_status st = GQT_OK;
+  Workspace& ws = *h->ws;
+  bool changed = false;
+  for (int k = 0; k < n_candidates && st == GQT_OK; ++k) {
+    const int V = candidates[k];
+    double rate = 0.0;
+    if (form_ops(precision, V)) {
+      gqt_vec* x = nullptr;
+      double2* mu = nullptr;
+      st = gqt_vec_create(h->n, V, precision, &x);
+      if (st == GQT_OK) {
+        const size_t bytes = (size_t)n_moments * h->n_real * V * sizeof(double2);
+        cudaError_t ce = cudaMalloc(&mu, bytes);
+        if (ce != cudaSuccess)
+          st = cuda_fail(ce, "cudaMalloc(probe moments)", __FILE__, __LINE__);
+      }
+      // Shapes: vectors per thread 4 (the default) and 2, where the form has both.
+      const int shapes[2] = {0, 2};
+      const int n_shapes = (precision == GQT_FP32 && V >= 4) ? 2 : 1;
+      int best_w = 0;
+      for (int si = 0; si < n_shapes && st == GQT_OK; ++si) {
+        h->wpt[V] = shapes[si];
+        st = gqt_moments_device(h, x, x, n_moments, mu);  // warm-up, graph capture
+        float ms = 0.f;
+        if (st == GQT_OK) {
+          cudaEventRecord(e0, s);
+          st = gqt_moments_device(h, x, x, n_moments, mu);
+          if (st == GQT_OK)
+            st = gqt_moments_device(h, x, x, n_moments, mu);
+          cudaEventRecord(e1, s);
+          cudaError_t ce = cudaEventSynchronize(e1);
+          if (ce == cudaSuccess)
+            ce = cudaEventElapsedTime(&ms, e0, e1);
+          if (st == GQT_OK && ce != cudaSuccess)
+            st = cuda_fail(ce, "autotune timing", __FILE__, __LINE__);
+        }
+        const double r = (st == GQT_OK && ms > 0.f)
+                           ? 2.0 * (double)V * (double)sites * n_moments / (ms * 1e-3)
+                           : 0.0;
+        if (r > rate) {
+          rate = r;
+          best_w = shapes[si];
+        }
+        // The probe's graph was captured with this shape; drop it before the next.
+        cudaStreamSynchronize(s);
+        for (auto it = ws.graphs.begin(); it != ws.graphs.end();) {
+          if (x && std::get<0>(it->first) == x->data) {
+            cudaGraphExecDestroy(it->second);
+            it = ws.graphs.erase(it);
+          } else {
+            ++it;
+          }
+        }
+      }
+      if (h->wpt[V] != best_w || n_shapes > 1)
+        changed = true;
+      h->wpt[V] = best_w;
+      cudaFree(mu);
+      gqt_vec_destroy(x);
+    }
+    if (rates)
+      rates[k] = rate;
+    if (rate > best_rate) {
+      best_rate = rate;
+      *best = V;
+    }
+  }
+  if (changed) {
+    // Graphs captured before the tuning launch the old shapes; recapture on next use.
+    cudaStreamSynchronize(s);
+    for (auto& kv : ws.graphs)
+      cudaGraphExecDestroy(kv.second);
+    ws.graphs.clear();
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != GQT_OK)
+    return st;
+  if (best_rate <= 0.0)
+    return fail(GQT_ERR_ARG, "%s: no candidate is a supported vector count", w);
   return GQT_OK;
 }

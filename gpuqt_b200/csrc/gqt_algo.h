@@ -34,6 +34,6 @@ Workspace* new_workspace();
 
 // The i-th temporary vector of a form (n * nvec elements of elem bytes).
 gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i, void** out);
-gqt_status ws_dot(Workspace& ws, int nvec, DotScratch** out);
+gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out);
 
 }  // namespace gqt

@@ -18,6 +18,10 @@ struct FormOps {
   gqt_status (*step)(const Op& op, int mode, const void* t0, const void* t1, void* out,
                      const void* left, const Dot* dot);
   gqt_status (*dot)(size_t total, const void* state, const void* left, const Dot& dot);
+  // One step of a realisation batch (mode kDotOnly, kApply or kCheb) with moments per
+  // realisation.
+  gqt_status (*step_multi)(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                           const void* left, const MultiDot& md);
   gqt_status (*xop)(const Op& op, bool current, const void* in, void* out);
   // Evolution terms; out is a double2 accumulator (the FP64 state itself, or the
   // FP32 form's FP64 accumulator).

@@ -33,6 +33,16 @@ gqt_status launch(K* kernel, size_t total, Args... args)
   return GQT_OK;
 }
 
+template <typename K, typename... Args>
+gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
+{
+  const int grid = grid_for((const void*)kernel, total);
+  kernel<<<grid, kBlock, smem, stream()>>>(args...);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
 // Vectors a thread advances per step launch: 4 float2 (two 16-byte loads) or 2 double2.
 template <typename VT2, int V>
 constexpr int vectors_per_thread()
@@ -43,7 +53,10 @@ constexpr int vectors_per_thread()
 
 template <typename VT2, int V, class A>
 struct FormImpl {
+  // Default vectors per thread, and the alternative the autotuner may choose (two
+  // vectors per thread: half the accumulator registers, twice the threads per site).
   static constexpr int W = vectors_per_thread<VT2, V>();
+  static constexpr int W2 = (std::is_same<VT2, float2>::value && V >= 4) ? 2 : W;
 
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)
@@ -58,15 +71,25 @@ struct FormImpl {
       constexpr int Z = decltype(zc)::value;
       if constexpr (W > 1) {
         // several vectors per thread: one launch item per (site, W vectors)
-        const size_t items = (size_t)op.n * (V / W);
-        if (mode == kApply) {
+        auto run = [&](auto wc) -> gqt_status {
+          constexpr int WW = decltype(wc)::value;
+          const size_t items = (size_t)op.n * (V / WW);
+          if (mode == kApply) {
+            if (dot)
+              return launch(k_step_vec<VT2, V, WW, Z, A, kApply, true>, items, op, a0, a1, o, l,
+                            d);
+            return launch(k_step_vec<VT2, V, WW, Z, A, kApply, false>, items, op, a0, a1, o, l,
+                          d);
+          }
           if (dot)
-            return launch(k_step_vec<VT2, V, W, Z, A, kApply, true>, items, op, a0, a1, o, l, d);
-          return launch(k_step_vec<VT2, V, W, Z, A, kApply, false>, items, op, a0, a1, o, l, d);
+            return launch(k_step_vec<VT2, V, WW, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
+          return launch(k_step_vec<VT2, V, WW, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
+        };
+        if constexpr (W2 != W) {
+          if (op.wpt == W2)
+            return run(std::integral_constant<int, W2>{});
         }
-        if (dot)
-          return launch(k_step_vec<VT2, V, W, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
-        return launch(k_step_vec<VT2, V, W, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
+        return run(std::integral_constant<int, W>{});
       }
       if (mode == kApply) {
         if (dot)
@@ -77,6 +100,44 @@ struct FormImpl {
         return launch(k_step<VT2, V, Z, A, kCheb, true>, total, op, a0, a1, o, l, d);
       return launch(k_step<VT2, V, Z, A, kCheb, false>, total, op, a0, a1, o, l, d);
     });
+  }
+
+  static gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1,
+                               void* out, const void* left, const MultiDot& md_in)
+  {
+    const VT2* a0 = (const VT2*)t0;
+    const VT2* a1 = (const VT2*)t1;
+    VT2* o = (VT2*)out;
+    const VT2* l = (const VT2*)left;
+    MultiDot md = md_in;
+    const size_t items = (size_t)md.n_tiles * kBlock;
+    GQT_TRY(with_z(op.z, [&](auto zc) -> gqt_status {
+      constexpr int Z = decltype(zc)::value;
+      auto go = [&](auto* kernel) -> gqt_status {
+        md.blocks = grid_for((const void*)kernel, items);
+        kernel<<<md.blocks, kBlock, 0, stream()>>>(op, a0, a1, o, l, md);
+        count_launches(1);
+        GQT_CUDA(cudaGetLastError());
+        return GQT_OK;
+      };
+      auto pick = [&](auto wc) -> gqt_status {
+        constexpr int WW = decltype(wc)::value;
+        if (mode == kDotOnly)
+          return go(k_step_multi<VT2, V, WW, Z, A, kDotOnly>);
+        if (mode == kApply)
+          return go(k_step_multi<VT2, V, WW, Z, A, kApply>);
+        return go(k_step_multi<VT2, V, WW, Z, A, kCheb>);
+      };
+      if constexpr (W2 != W) {
+        if (op.wpt == W2)
+          return pick(std::integral_constant<int, W2>{});
+      }
+      return pick(std::integral_constant<int, W>{});
+    }));
+    k_tile_reduce<V><<<md.n_real * V, kBlock, 0, stream()>>>(md);
+    count_launches(1);
+    GQT_CUDA(cudaGetLastError());
+    return GQT_OK;
   }
 
   static gqt_status dot(size_t total, const void* state, const void* left, const Dot& d)
@@ -153,7 +214,7 @@ struct FormImpl {
 
   static const FormOps* table(int precision)
   {
-    static const FormOps t = {precision, V,      sizeof(VT2), step,     dot,      xop,
+    static const FormOps t = {precision, V,      sizeof(VT2), step,  dot, step_multi, xop,
                               cheb01,    cheb2,  cheb1x,      cheb2x,   add,      apply_sz,
                               interleave, deinterleave};
     return &t;

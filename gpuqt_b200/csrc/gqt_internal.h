@@ -74,6 +74,17 @@ struct gqt_ham {
   double* xx = nullptr;     // [z*n] column-major
   double* pot = nullptr;    // [n]
   bool has_xx = false;
+  // Realisation batch (gqt_ham_create_batch): n_real > 1 block-diagonal models, each
+  // padded to whole tiles and pre-divided by its own E_max (energy_max is then 1).
+  int n_real = 1;
+  int tile_sites = 0;
+  int n_tiles = 0;
+  int* tile_first = nullptr;  // device, [n_real + 1]: first tile of each model
+  std::vector<int> real_offset, real_n;
+  std::vector<double> real_emax;
+  // Vectors per thread of the batched step for each vector count (0: the form's
+  // default); set by the autotuner.
+  mutable int wpt[33] = {};
   std::unique_ptr<gqt::Workspace> ws;
   ~gqt_ham();
 };

@@ -41,6 +41,7 @@ struct Op {
   const double* __restrict__ xx;
   double emax;
   double inv_emax;
+  int wpt;  // vectors per thread chosen for this launch (0: the form's default)
 };
 
 struct Dot {
@@ -210,8 +211,27 @@ __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const
 
   // Last block: thread t sums blocks t/V, t/V + kBlock/V, ... of vector t % V.
   const int v = threadIdx.x % V;
+  constexpr int kStride = kBlock / V;
   CSum r{0.0, 0.0}, i{0.0, 0.0};
-  for (int b = threadIdx.x / V; b < (int)gridDim.x; b += kBlock / V) {
+  int b = threadIdx.x / V;
+  // Four blocks' partials are loaded before they are merged (in block order), so the
+  // L2 round trips overlap.
+  for (; b + 3 * kStride < (int)gridDim.x; b += 4 * kStride) {
+    double q[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double* p = dot.partials + ((size_t)(b + u * kStride) * V + v) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        q[u][k] = __ldcg(p + k);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      csum_merge(r, CSum{q[u][0], q[u][1]});
+      csum_merge(i, CSum{q[u][2], q[u][3]});
+    }
+  }
+  for (; b < (int)gridDim.x; b += kStride) {
     const double* p = dot.partials + ((size_t)b * V + v) * 4;
     csum_merge(r, CSum{__ldcg(p + 0), __ldcg(p + 1)});
     csum_merge(i, CSum{__ldcg(p + 2), __ldcg(p + 3)});
@@ -461,6 +481,225 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
   }
   if constexpr (DOT)
     dot_finish_w<V, W>(re, im, dot);
+}
+
+// ------------------------------------------------------------------ realisation batches
+// A batch is a block-diagonal operator of R independent models (disorder realisations
+// of uneven lattice sizes), each padded to whole tiles of `tile_sites` sites and with
+// its operator pre-divided by its own E_max. Moments are kept per realisation.
+struct MultiDot {
+  double* partials;        // [blocks][R][V][4]: each block's sums per realisation
+  double2* mu;             // this moment's R * V results, [r][v]
+  const int* tile_first;   // [R + 1]: realisation r owns tiles [tile_first[r], tile_first[r+1])
+  int n_tiles;
+  int tile_sites;
+  int n_real;
+  int blocks;              // grid of the step launch
+};
+
+enum { kDotOnly = 2 };
+
+// Threads < V receive the block sum of vector threadIdx.x (W vectors per thread,
+// v0 = (lane % (V/W)) * W). Every thread must call it; it synchronises twice.
+template <int V, int W>
+__device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSum& out_re,
+                                               CSum& out_im, double (*sh)[V][4])
+{
+  constexpr int kTps = V / W;
+  constexpr int kWarps = kBlock / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off >= kTps; off >>= 1) {
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      csum_merge(re[k], shfl_xor(re[k], off));
+      csum_merge(im[k], shfl_xor(im[k], off));
+    }
+  }
+  if (lane < kTps) {
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+      sh[warp][lane * W + k][0] = re[k].s;
+      sh[warp][lane * W + k][1] = re[k].c;
+      sh[warp][lane * W + k][2] = im[k].s;
+      sh[warp][lane * W + k][3] = im[k].c;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < V) {
+    const int v = threadIdx.x;
+    out_re = CSum{sh[0][v][0], sh[0][v][1]};
+    out_im = CSum{sh[0][v][2], sh[0][v][3]};
+    for (int w = 1; w < kWarps; ++w) {
+      csum_merge(out_re, CSum{sh[w][v][0], sh[w][v][1]});
+      csum_merge(out_im, CSum{sh[w][v][2], sh[w][v][3]});
+    }
+  }
+  __syncthreads();
+}
+
+// One Chebyshev step (or moment 0 / moment 1) over every realisation of a batch.
+// Block b takes the contiguous, balanced tile range [b*T/G, (b+1)*T/G); a tile is
+// 256 sites, so one block round of 256 threads never straddles two realisations.
+// Per-thread sums are reduced over the block only when the range moves on to the
+// next realisation (once or twice per step for most blocks) and written to the
+// block's slot of that realisation; slots of realisations outside the range are
+// zeroed. k_tile_reduce then sums the blocks per realisation in fixed order.
+template <typename VT2, int V, int W, int Z, class A, int MODE>
+__global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
+                                                       const VT2* __restrict__ t1, VT2* out,
+                                                       const VT2* __restrict__ left, MultiDot md)
+{
+  constexpr int kTps = V / W;
+  constexpr int kWarps = kBlock / 32;
+  constexpr bool kExact = std::is_same<A, ExactArith>::value;
+  __shared__ double sh[kWarps][V][4];
+  const int R = md.n_real;
+  const int t_begin = (int)((long long)blockIdx.x * md.n_tiles / gridDim.x);
+  const int t_end = (int)((long long)(blockIdx.x + 1) * md.n_tiles / gridDim.x);
+  const size_t items_per_tile = (size_t)md.tile_sites * kTps;
+  double* slots = md.partials + (size_t)blockIdx.x * R * V * 4;
+  int r = 0;
+  while (r + 1 < R && md.tile_first[r + 1] <= t_begin)
+    ++r;
+  const int r_begin = r;
+  CSum re[W], im[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    re[k] = im[k] = CSum{0.0, 0.0};
+
+  auto flush = [&](int rr) {
+    CSum br{0.0, 0.0}, bi{0.0, 0.0};
+    block_reduce_w<V, W>(re, im, br, bi, sh);
+    if (threadIdx.x < V) {
+      double* q = slots + ((size_t)rr * V + threadIdx.x) * 4;
+      q[0] = br.s;
+      q[1] = br.c;
+      q[2] = bi.s;
+      q[3] = bi.c;
+    }
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      re[k] = im[k] = CSum{0.0, 0.0};
+  };
+
+  for (int t = t_begin; t < t_end; ++t) {
+    if (t >= md.tile_first[r + 1]) {  // block-uniform: the range enters the next model
+      flush(r);
+      while (t >= md.tile_first[r + 1])
+        ++r;
+    }
+    for (size_t it = threadIdx.x; it < items_per_tile; it += kBlock) {
+      const size_t g = (size_t)t * items_per_tile + it;
+      const int i = (int)(g / kTps);
+      const int v0 = (int)(g % kTps) * W;
+      const size_t base = (size_t)i * V + v0;
+      double2 r2[W];
+      if constexpr (MODE == kDotOnly) {
+        ldw<W>(t1 + base, r2);
+      } else {
+        const double p = op.pot[i];
+        double2 x[W];
+        ldw<W>(t1 + base, x);
+        double tr[W], ti[W];
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          tr[k] = A::mul(p, x[k].x);
+          ti[k] = A::mul(p, x[k].y);
+        }
+        const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+        auto body = [&](int m) {
+          const size_t e = (size_t)m * op.n + i;
+          const int j = op.nl[e];
+          const double2 h = op.hop[e];
+          double2 y[W];
+          ldw<W>(t1 + (size_t)j * V + v0, y);
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+            ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+          }
+        };
+        if constexpr (Z > 0) {
+#pragma unroll
+          for (int m = 0; m < Z; ++m)
+            if (m < cnt)
+              body(m);
+        } else {
+          for (int m = 0; m < cnt; ++m)
+            body(m);
+        }
+        if constexpr (MODE == kCheb) {
+          double2 y0[W];
+          ldw<W>(t0 + base, y0);
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            r2[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0[k].x),
+                                 A::two_x_minus(A::scale(ti[k], op), y0[k].y));
+        } else {
+#pragma unroll
+          for (int k = 0; k < W; ++k)
+            r2[k] = make_double2(A::scale(tr[k], op), A::scale(ti[k], op));
+        }
+        stw<W>(out + base, r2);
+      }
+      double2 l[W];
+      ldw<W>(left + base, l);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        if constexpr (kExact) {
+          dot_term(re[k], im[k], MODE == kDotOnly ? r2[k] : stored(out, r2[k]), l[k]);
+        } else {
+          re[k].s = fma(r2[k].x, l[k].x, fma(r2[k].y, l[k].y, re[k].s));
+          im[k].s = fma(r2[k].y, l[k].x, fma(-r2[k].x, l[k].y, im[k].s));
+        }
+      }
+    }
+  }
+  flush(r);
+  // Realisations this block never reached get zero sums.
+  for (int k = threadIdx.x; k < R * V * 4; k += kBlock) {
+    const int rr = k / (V * 4);
+    if (rr < r_begin || rr > r || t_begin >= t_end)
+      slots[k] = 0.0;
+  }
+}
+
+// Per-realisation moments of a batch step: block p sums the slots of pair
+// p = (r, v) over the step's blocks in fixed order and writes mu[p].
+template <int V>
+__global__ void __launch_bounds__(kBlock) k_tile_reduce(MultiDot md)
+{
+  const int p = blockIdx.x;
+  const int pairs = md.n_real * V;
+  CSum re{0.0, 0.0}, im{0.0, 0.0};
+  for (int b = threadIdx.x; b < md.blocks; b += kBlock) {
+    const double* q = md.partials + ((size_t)b * pairs + p) * 4;
+    csum_merge(re, CSum{q[0], q[1]});
+    csum_merge(im, CSum{q[2], q[3]});
+  }
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    csum_merge(re, shfl_xor(re, off));
+    csum_merge(im, shfl_xor(im, off));
+  }
+  __shared__ double sh[kBlock / 32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    sh[warp][0] = re.s;
+    sh[warp][1] = re.c;
+    sh[warp][2] = im.s;
+    sh[warp][3] = im.c;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    CSum a{sh[0][0], sh[0][1]}, b{sh[0][2], sh[0][3]};
+    for (int w = 1; w < kBlock / 32; ++w) {
+      csum_merge(a, CSum{sh[w][0], sh[w][1]});
+      csum_merge(b, CSum{sh[w][2], sh[w][3]});
+    }
+    md.mu[p] = make_double2(__dadd_rn(a.s, a.c), __dadd_rn(b.s, b.c));
+  }
 }
 
 // [X,H] in / E_max (src/hamiltonian.cu:240-271) or V in = -i sum H xx in

@@ -324,88 +324,220 @@ gqt_ham::~gqt_ham()
   cudaFree(hop);
   cudaFree(xx);
   cudaFree(pot);
+  cudaFree(tile_first);
 }
 
-extern "C" gqt_status gqt_ham_create(const gqt_ell_desc* d, gqt_ham** out)
+namespace {
+
+// Host checks of one model's ELL arrays, before anything reaches the device.
+gqt_status validate_desc(const gqt_ell_desc* d, const char* what)
 {
-  if (!d || !out)
-    return fail(GQT_ERR_ARG, "gqt_ham_create: null argument");
-  *out = nullptr;
+  if (!d)
+    return fail(GQT_ERR_ARG, "%s: null descriptor", what);
   const int n = d->n, z = d->max_neighbor;
   if (n <= 0)
-    return fail(GQT_ERR_ARG, "gqt_ham_create: number of sites must be > 0 (got %d)", n);
+    return fail(GQT_ERR_ARG, "%s: number of sites must be > 0 (got %d)", what, n);
   if (z <= 0)
-    return fail(GQT_ERR_ARG, "gqt_ham_create: max_neighbor must be > 0 (got %d)", z);
+    return fail(GQT_ERR_ARG, "%s: max_neighbor must be > 0 (got %d)", what, z);
   if (!(d->energy_max > 0.0))
-    return fail(GQT_ERR_ARG, "gqt_ham_create: energy_max must be > 0 (got %g)", d->energy_max);
+    return fail(GQT_ERR_ARG, "%s: energy_max must be > 0 (got %g)", what, d->energy_max);
   if (!d->neighbor_number || !d->neighbor_list || !d->potential || !d->hopping_real ||
       !d->hopping_imag)
-    return fail(GQT_ERR_ARG, "gqt_ham_create: null ELL array");
-  const size_t pairs = (size_t)n * z;
-  if (pairs > (size_t)1 << 40)
-    return fail(GQT_ERR_ARG, "gqt_ham_create: n * max_neighbor too large");
-
-  // Validate on the host before anything reaches the device, then transpose to the
-  // column-major [m*n + i] layout (the transpose of src/hamiltonian.cu:47-88).
-  int uniform = 1;
+    return fail(GQT_ERR_ARG, "%s: null ELL array", what);
+  if ((size_t)n * z > (size_t)1 << 40)
+    return fail(GQT_ERR_ARG, "%s: n * max_neighbor too large", what);
   for (int i = 0; i < n; ++i) {
     const int c = d->neighbor_number[i];
     if (c < 0 || c > z)
-      return fail(GQT_ERR_INPUT, "gqt_ham_create: site %d has %d neighbours (max_neighbor %d)",
-                  i, c, z);
-    if (c != z)
-      uniform = 0;
+      return fail(GQT_ERR_INPUT, "%s: site %d has %d neighbours (max_neighbor %d)", what, i, c,
+                  z);
     for (int m = 0; m < c; ++m) {
       const int j = d->neighbor_list[(size_t)i * z + m];
       if (j < 0 || j >= n)
-        return fail(GQT_ERR_INPUT, "gqt_ham_create: site %d neighbour %d index %d out of [0, %d)",
-                    i, m, j, n);
+        return fail(GQT_ERR_INPUT, "%s: site %d neighbour %d index %d out of [0, %d)", what, i,
+                    m, j, n);
     }
   }
-  std::vector<int> nl(pairs, 0);
-  std::vector<double2> hop(pairs, make_double2(0.0, 0.0));
-  std::vector<double> xx(pairs, 0.0);
+  return GQT_OK;
+}
+
+// Column-major ELL arrays of the whole (possibly batched) operator on the host.
+struct Packed {
+  int n = 0, z = 0;
+  bool uniform = true;
+  std::vector<int> nn, nl;
+  std::vector<double2> hop;
+  std::vector<double> xx, pot;
+  void init(int n_, int z_)
+  {
+    n = n_;
+    z = z_;
+    nn.assign(n, z);
+    nl.assign((size_t)n * z, 0);
+    hop.assign((size_t)n * z, make_double2(0.0, 0.0));
+    xx.assign((size_t)n * z, 0.0);
+    pot.assign(n, 0.0);
+    // Rows start as padding: full length, pointing at the site itself, zero hopping.
+    for (int m = 0; m < z; ++m)
+      for (int i = 0; i < n; ++i)
+        nl[(size_t)m * n + i] = i;
+  }
+};
+
+// Copies one model into sites [base, base + d->n) of P (the transpose of
+// src/hamiltonian.cu:47-88). With divide = false the values are copied bit for bit;
+// with divide = true the hoppings and potentials are divided by the model's E_max.
+void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
+{
+  const int n = d->n, z = d->max_neighbor;
+  const double e = d->energy_max;
   for (int i = 0; i < n; ++i) {
     const int c = d->neighbor_number[i];
+    const int row = base + i;
+    P.nn[row] = c;
+    if (c != P.z)
+      P.uniform = false;
     for (int m = 0; m < c; ++m) {
-      const size_t src = (size_t)i * z + m, dst = (size_t)m * n + i;
-      nl[dst] = d->neighbor_list[src];
-      hop[dst] = make_double2(d->hopping_real[src], d->hopping_imag[src]);
+      const size_t src = (size_t)i * z + m, dst = (size_t)m * P.n + row;
+      P.nl[dst] = base + d->neighbor_list[src];
+      P.hop[dst] = divide ? make_double2(d->hopping_real[src] / e, d->hopping_imag[src] / e)
+                          : make_double2(d->hopping_real[src], d->hopping_imag[src]);
       if (d->xx)
-        xx[dst] = d->xx[src];
+        P.xx[dst] = d->xx[src];
     }
-    // Padding entries point at the site itself with zero hopping; they are never
-    // read (the row length bounds every loop) but keep gathers in bounds.
-    for (int m = c; m < z; ++m)
-      nl[(size_t)m * n + i] = i;
+    // Short rows: the entries past the row length are never read (the row length
+    // bounds every loop) but point at the site itself so gathers stay in bounds.
+    for (int m = c; m < P.z; ++m)
+      P.nl[(size_t)m * P.n + row] = row;
+    P.pot[row] = divide ? d->potential[i] / e : d->potential[i];
   }
+}
 
-  auto h = new (std::nothrow) gqt_ham;
-  if (!h)
-    return fail(GQT_ERR_ALLOC, "gqt_ham_create: host allocation failed");
-  std::unique_ptr<gqt_ham> guard(h);
-  h->n = n;
-  h->z = z;
-  h->energy_max = d->energy_max;
-  h->uniform = uniform;
-  h->has_xx = d->xx != nullptr;
+gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
+{
+  const size_t pairs = (size_t)P.n * P.z;
+  h->n = P.n;
+  h->z = P.z;
+  h->energy_max = energy_max;
+  h->uniform = P.uniform ? 1 : 0;
+  h->has_xx = has_xx;
   cudaGetDevice(&h->device);
   GQT_CUDA(cudaMalloc(&h->nl, pairs * sizeof(int)));
   GQT_CUDA(cudaMalloc(&h->hop, pairs * sizeof(double2)));
   GQT_CUDA(cudaMalloc(&h->xx, pairs * sizeof(double)));
-  GQT_CUDA(cudaMalloc(&h->pot, (size_t)n * sizeof(double)));
-  if (!uniform) {
-    GQT_CUDA(cudaMalloc(&h->nn, (size_t)n * sizeof(int)));
-    GQT_CUDA(cudaMemcpy(h->nn, d->neighbor_number, (size_t)n * sizeof(int),
-                        cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMalloc(&h->pot, (size_t)P.n * sizeof(double)));
+  if (!P.uniform) {
+    GQT_CUDA(cudaMalloc(&h->nn, (size_t)P.n * sizeof(int)));
+    GQT_CUDA(cudaMemcpy(h->nn, P.nn.data(), (size_t)P.n * sizeof(int), cudaMemcpyHostToDevice));
   }
-  GQT_CUDA(cudaMemcpy(h->nl, nl.data(), pairs * sizeof(int), cudaMemcpyHostToDevice));
-  GQT_CUDA(cudaMemcpy(h->hop, hop.data(), pairs * sizeof(double2), cudaMemcpyHostToDevice));
-  GQT_CUDA(cudaMemcpy(h->xx, xx.data(), pairs * sizeof(double), cudaMemcpyHostToDevice));
-  GQT_CUDA(cudaMemcpy(h->pot, d->potential, (size_t)n * sizeof(double),
+  GQT_CUDA(cudaMemcpy(h->nl, P.nl.data(), pairs * sizeof(int), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->hop, P.hop.data(), pairs * sizeof(double2), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->xx, P.xx.data(), pairs * sizeof(double), cudaMemcpyHostToDevice));
+  GQT_CUDA(cudaMemcpy(h->pot, P.pot.data(), (size_t)P.n * sizeof(double),
                       cudaMemcpyHostToDevice));
   h->ws.reset(new_workspace());
+  return GQT_OK;
+}
+
+}  // namespace
+
+extern "C" gqt_status gqt_ham_create(const gqt_ell_desc* d, gqt_ham** out)
+{
+  if (!out)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: null argument");
+  *out = nullptr;
+  if (!d)
+    return fail(GQT_ERR_ARG, "gqt_ham_create: null argument");
+  GQT_TRY(validate_desc(d, "gqt_ham_create"));
+  Packed P;
+  P.init(d->n, d->max_neighbor);
+  pack_desc(d, 0, false, P);
+  auto h = new (std::nothrow) gqt_ham;
+  if (!h)
+    return fail(GQT_ERR_ALLOC, "gqt_ham_create: host allocation failed");
+  std::unique_ptr<gqt_ham> guard(h);
+  GQT_TRY(upload_packed(P, d->energy_max, d->xx != nullptr, h));
+  h->real_offset = {0, d->n};
+  h->real_n = {d->n};
+  h->real_emax = {d->energy_max};
   *out = guard.release();
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count, gqt_ham** out)
+{
+  const char* w = "gqt_ham_create_batch";
+  if (!out || !descs)
+    return fail(GQT_ERR_ARG, "%s: null argument", w);
+  *out = nullptr;
+  if (count < 1 || count > GQT_MAX_REALISATIONS)
+    return fail(GQT_ERR_ARG, "%s: count must be 1..%d (got %d)", w, GQT_MAX_REALISATIONS,
+                count);
+  const int tile = GQT_BATCH_TILE_SITES;
+  long long total = 0;
+  int zmax = 0;
+  std::vector<int> offset(count + 1, 0);
+  for (int r = 0; r < count; ++r) {
+    GQT_TRY(validate_desc(&descs[r], w));
+    offset[r] = (int)total;
+    total += ((long long)descs[r].n + tile - 1) / tile * tile;
+    zmax = descs[r].max_neighbor > zmax ? descs[r].max_neighbor : zmax;
+    if (total * zmax > (long long)1 << 40 || total > 2000000000LL)
+      return fail(GQT_ERR_ARG, "%s: batch too large", w);
+  }
+  offset[count] = (int)total;
+  Packed P;
+  P.init((int)total, zmax);
+  for (int r = 0; r < count; ++r)
+    pack_desc(&descs[r], offset[r], true, P);
+  auto h = new (std::nothrow) gqt_ham;
+  if (!h)
+    return fail(GQT_ERR_ALLOC, "%s: host allocation failed", w);
+  std::unique_ptr<gqt_ham> guard(h);
+  bool has_xx = true;
+  for (int r = 0; r < count; ++r)
+    has_xx = has_xx && descs[r].xx != nullptr;
+  // Each model is pre-divided by its own E_max, so the operator is applied with 1.
+  GQT_TRY(upload_packed(P, 1.0, has_xx, h));
+  h->n_real = count;
+  h->tile_sites = tile;
+  h->n_tiles = (int)(total / tile);
+  h->real_offset = offset;
+  for (int r = 0; r < count; ++r) {
+    h->real_n.push_back(descs[r].n);
+    h->real_emax.push_back(descs[r].energy_max);
+  }
+  std::vector<int> first(count + 1);
+  for (int r = 0; r <= count; ++r)
+    first[r] = offset[r] / tile;
+  GQT_CUDA(cudaMalloc(&h->tile_first, first.size() * sizeof(int)));
+  GQT_CUDA(cudaMemcpy(h->tile_first, first.data(), first.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  *out = guard.release();
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_realisations(const gqt_ham* h, int* count)
+{
+  if (!h || !count)
+    return fail(GQT_ERR_ARG, "gqt_ham_realisations: null argument");
+  *count = h->n_real;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
+                                          double* energy_max)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_realisation: null handle");
+  if (r < 0 || r >= h->n_real)
+    return fail(GQT_ERR_ARG, "gqt_ham_realisation: index %d outside 0..%d", r, h->n_real - 1);
+  if (offset)
+    *offset = h->real_offset[r];
+  if (n)
+    *n = h->real_n[r];
+  if (energy_max)
+    *energy_max = h->real_emax[r];
   return GQT_OK;
 }
 

@@ -22,10 +22,12 @@ from . import workloads as W
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--workload", default="graphene2m", choices=sorted(W.CONFIGS))
+    ap.add_argument("--workload", default="graphene2m", choices=sorted(W.CONFIGS) + ["batch"])
     ap.add_argument("--form", default="fp64")
     ap.add_argument("--moments", type=int, default=20)
     ap.add_argument("--sets", type=int, default=2)
+    ap.add_argument("--autotune", action="store_true",
+                    help="let the autotuner pick the shape for this vector count first")
     args = ap.parse_args()
 
     import torch
@@ -39,12 +41,28 @@ def main() -> None:
     V = int(mo.group(2) or 1)
     tmp = tempfile.mkdtemp(prefix="gqt_prof_")
     try:
-        m = g.Model.load(W.config_dir(tmp, args.workload))
-        H = g.Hamiltonian(m)
-        vecs = [m.initial_state() for _ in range(V)]
-        X = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
-                               nvec=V, precision=prec)
-        mu = torch.empty(2 * args.moments * V, dtype=torch.float64, device="cuda")
+        if args.workload == "batch":
+            models = [g.Model.load(d) for d in W.batch_dirs(tmp, moments=args.moments)]
+            H = g.Hamiltonian.batch(models)
+            rng = np.random.default_rng(1)
+            per = []
+            for mm in models:
+                ph = rng.uniform(0.0, 2 * np.pi, size=(V, mm.n))
+                per.append((np.cos(ph), np.sin(ph)))
+            X = g.Vector.from_host(*H.scatter(per), nvec=V, precision=prec)
+            sites = sum(mm.n for mm in models)
+        else:
+            m = g.Model.load(W.config_dir(tmp, args.workload))
+            H = g.Hamiltonian(m)
+            vecs = [m.initial_state() for _ in range(V)]
+            X = g.Vector.from_host(np.stack([v[0] for v in vecs]),
+                                   np.stack([v[1] for v in vecs]), nvec=V, precision=prec)
+            sites = m.n
+        tuned = None
+        if args.autotune:
+            tuned = g.autotune_nvec(H, prec, 20, [V])[1]
+        R = getattr(H, "n_real", 1)
+        mu = torch.empty(2 * args.moments * V * R, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream()
         g.set_stream(stream.cuda_stream)
         g.moments_device(H, X, X, args.moments, mu.data_ptr())
@@ -56,9 +74,9 @@ def main() -> None:
         b.record(stream)
         torch.cuda.synchronize()
         s = a.elapsed_time(b) / 1e3
-        print(json.dumps({"workload": args.workload, "form": args.form, "sites": m.n,
-                          "moments": args.moments, "sets": args.sets,
-                          "site_moments_per_s": V * m.n * args.moments * args.sets / s}))
+        print(json.dumps({"workload": args.workload, "form": args.form, "sites": sites,
+                          "moments": args.moments, "sets": args.sets, "autotune": tuned,
+                          "site_moments_per_s": V * sites * args.moments * args.sets / s}))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
 

@@ -97,6 +97,10 @@ CONFIGS = {
         moments=5000, time_step=[FS] * 20, calculate=("vac",), seed=5,
         description="honeycomb graphene 4,194,304 sites, t=-2.7 eV, W=1.5 eV (seed 5), "
                     "E_max 9.0, 5000 moments"),
+    "square1m": dict(
+        kind="square", cells=(1024, 1024, 1), hopping=-1.0, anderson=2.0, energy_max=5.2,
+        moments=2000, time_step=[1.0], calculate=(), seed=17,
+        description="square 1024x1024 = 1,048,576 sites, z=4, t=-1, W=2 (seed 17), E_max 5.2"),
     "cubic256": dict(
         kind="cubic", cells=(256, 256, 256), hopping=-1.0, anderson=16.5, energy_max=15.0,
         moments=4000, time_step=[1.0] * 30, calculate=("vac", "msd"), seed=13,
@@ -116,3 +120,24 @@ def config_sites(name: str) -> int:
     c = CONFIGS[name]
     per_cell = 4 if c["kind"] == "graphene" else 1
     return per_cell * int(np.prod(c["cells"]))
+
+
+def batch_realisations(count: int = 8, seed: int = 11):
+    """The realisation batch: square lattices L x L with log-uniform L in [128, 2048]
+    (L = round(2^u), u ~ U(7, 11)), Anderson W ~ U(0.5, 4), E_max = 4 + W/2 + 0.1,
+    hopping -1. Drawn from numpy's MT19937 (RandomState(seed))."""
+    rs = np.random.RandomState(seed)
+    u = rs.uniform(7.0, 11.0, count)
+    w = rs.uniform(0.5, 4.0, count)
+    return [dict(L=int(round(2.0 ** x)), W=float(ww), energy_max=4.0 + float(ww) / 2 + 0.1)
+            for x, ww in zip(u, w)]
+
+
+def batch_dirs(root: str, count: int = 8, seed: int = 11, moments: int = 2000):
+    """Input directories of the realisation batch (disorder seed seed + 1 + r)."""
+    out = []
+    for r, c in enumerate(batch_realisations(count, seed)):
+        out.append(write_input_dir(os.path.join(root, f"real{r}"), "square", (c["L"], c["L"], 1),
+                                   hopping=-1.0, anderson=c["W"], energy_max=c["energy_max"],
+                                   moments=moments, calculate=(), disorder_seed=seed + 1 + r))
+    return out

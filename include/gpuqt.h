@@ -85,6 +85,32 @@ gqt_status gqt_ham_destroy(gqt_ham* h);
 gqt_status gqt_ham_info(const gqt_ham* h, int* n, int* max_neighbor, int* uniform_rows,
                         double* energy_max);
 
+/* Realisation batches (no counterpart in the reference, which runs one model per
+ * process): `count` independent models — disorder realisations, lattices of uneven
+ * sizes — as one block-diagonal operator, so one launch per Chebyshev step advances
+ * all of them and all their vectors. Model r occupies sites
+ * [offset_r, offset_r + n_r) of the batch's vectors; each model is padded to a whole
+ * number of GQT_BATCH_TILE_SITES sites (padding sites carry zero vectors) and its
+ * operator is stored pre-divided by its own energy_max. On a batch, gqt_moments
+ * returns moments per model (layout [r][vector][m]); gqt_apply and
+ * gqt_kernel_polynomial apply the scaled operator; the evolution and current
+ * entry points are rejected (their Bessel coefficients depend on each model's
+ * energy_max). */
+#define GQT_BATCH_TILE_SITES 256
+#define GQT_MAX_REALISATIONS 32
+gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count, gqt_ham** out);
+gqt_status gqt_ham_realisations(const gqt_ham* h, int* count);
+gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
+                               double* energy_max);
+/* Project autotuner for the batched moment loop: times n_moments Chebyshev steps for
+ * each candidate number of vectors per launch (a supported nvec of `precision`) on
+ * this Hamiltonian and returns the one with the highest site-moments/s in *best
+ * (rates[k] receives candidate k's rate; may be NULL). Allocates and frees its own
+ * probe vectors. */
+gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_moments,
+                             const int* candidates, int n_candidates, int* best,
+                             double* rates);
+
 /* ---------------------------------------------------------------- vectors */
 /* Replaces Vector::Vector(int) (src/vector.cu:61-70): nvec vectors of n sites,
  * zero-initialised. precision is GQT_FP64 or GQT_FP32. */
@@ -162,7 +188,8 @@ gqt_status gqt_vec_segment_sum(const gqt_vec* in, int segment, int count, gqt_ve
 gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
                        int n_moments, double* mu_re, double* mu_im);
 /* As gqt_moments, but leaves the moments on the device (mu_dev: nvec*n_moments
- * double2 (re, im), moment-major [m*nvec + k]) and does not synchronise. */
+ * double2 (re, im), moment-major [m*nvec + k]; for a realisation batch
+ * [m][r][k], n_moments*count*nvec entries) and does not synchronise. */
 gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
                               int n_moments, void* mu_dev);
 /* Replaces evolve (src/sigma.cu:116-151): state <- U(direction * dt) state with
