@@ -81,3 +81,22 @@ def test_fp32_run_close_to_fp64(tmp_path):
         x, y = _read(str(b / f)), _read(str(a / f))
         for u, v in zip(x, y):
             assert np.max(np.abs(u - v)) <= 1e-5 * np.max(np.abs(v))
+
+
+def test_replica_launcher_matches_reference(tmp_path):
+    """torchrun -m gpuqt_b200.replicas (one rank here) against the reference's files."""
+    import socket
+    import sys
+    name = "chain_z2"
+    d = tmp_path / name
+    _copy_inputs(fixture_dir(name), d)
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    r = subprocess.run([sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+                        "--nproc-per-node=1", "--master-addr=127.0.0.1",
+                        f"--master-port={port}", "-m", "gpuqt_b200.replicas", str(d)],
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
+    for f in ("dos.out", "msd.out"):
+        _compare(str(d / f), os.path.join(REF, name, f))
