@@ -539,12 +539,13 @@ __device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSu
 }
 
 // One Chebyshev step (or moment 0 / moment 1) over every realisation of a batch.
-// Block b takes the contiguous, balanced tile range [b*T/G, (b+1)*T/G); a tile is
-// 256 sites, so one block round of 256 threads never straddles two realisations.
-// Per-thread sums are reduced over the block only when the range moves on to the
-// next realisation (once or twice per step for most blocks) and written to the
-// block's slot of that realisation; slots of realisations outside the range are
-// zeroed. k_tile_reduce then sums the blocks per realisation in fixed order.
+// Blocks take 256-site tiles grid-stride (tile t goes to block t % G), so the whole
+// GPU sweeps one compact wavefront and the neighbour gathers stay in L2; one block
+// round of 256 threads never straddles two realisations. A block's tiles come in
+// increasing order, so each realisation it meets is one contiguous run: per-thread
+// sums are reduced over the block when the run ends and written to the block's slot
+// of that realisation; slots of realisations it never meets are zeroed.
+// k_tile_reduce then sums the blocks per realisation in fixed order.
 template <typename VT2, int V, int W, int Z, class A, int MODE>
 __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
@@ -555,14 +556,10 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
   __shared__ double sh[kWarps][V][4];
   const int R = md.n_real;
-  const int t_begin = (int)((long long)blockIdx.x * md.n_tiles / gridDim.x);
-  const int t_end = (int)((long long)(blockIdx.x + 1) * md.n_tiles / gridDim.x);
   const size_t items_per_tile = (size_t)md.tile_sites * kTps;
   double* slots = md.partials + (size_t)blockIdx.x * R * V * 4;
   int r = 0;
-  while (r + 1 < R && md.tile_first[r + 1] <= t_begin)
-    ++r;
-  const int r_begin = r;
+  unsigned touched = 0u;  // realisations this block has written (R <= 32)
   CSum re[W], im[W];
 #pragma unroll
   for (int k = 0; k < W; ++k)
@@ -578,17 +575,21 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
       q[2] = bi.s;
       q[3] = bi.c;
     }
+    touched |= 1u << rr;
 #pragma unroll
     for (int k = 0; k < W; ++k)
       re[k] = im[k] = CSum{0.0, 0.0};
   };
 
-  for (int t = t_begin; t < t_end; ++t) {
-    if (t >= md.tile_first[r + 1]) {  // block-uniform: the range enters the next model
-      flush(r);
+  bool any = false;
+  for (int t = blockIdx.x; t < md.n_tiles; t += gridDim.x) {
+    if (t >= md.tile_first[r + 1]) {  // block-uniform: the next tile is in a later model
+      if (any)
+        flush(r);
       while (t >= md.tile_first[r + 1])
         ++r;
     }
+    any = true;
     for (size_t it = threadIdx.x; it < items_per_tile; it += kBlock) {
       const size_t g = (size_t)t * items_per_tile + it;
       const int i = (int)(g / kTps);
@@ -656,11 +657,12 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
       }
     }
   }
-  flush(r);
-  // Realisations this block never reached get zero sums.
+  if (any)
+    flush(r);
+  // Realisations this block never met get zero sums.
   for (int k = threadIdx.x; k < R * V * 4; k += kBlock) {
     const int rr = k / (V * 4);
-    if (rr < r_begin || rr > r || t_begin >= t_end)
+    if (!((touched >> rr) & 1u))
       slots[k] = 0.0;
   }
 }
