@@ -96,6 +96,9 @@ _SIGS = {
     "gqt_vec_segment_sum": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, _vp]),
     "gqt_moments": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _dp, _dp]),
     "gqt_moments_device": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, _vp]),
+    "gqt_moments_form": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    "gqt_moments_device_form": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
+    "gqt_vec_convert": (ctypes.c_int, [_vp, _vp]),
     "gqt_evolve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp]),
     "gqt_evolvex": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp]),
     "gqt_chebyshev_summation": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
@@ -208,6 +211,10 @@ class Vector:
 
     def copy_from(self, other: "Vector") -> None:
         _call("gqt_vec_copy", self.h, other.h)
+
+    def convert_from(self, other: "Vector") -> None:
+        """Copy across forms (FP64 <-> FP32)."""
+        _call("gqt_vec_convert", self.h, other.h)
 
     def add(self, other: "Vector") -> None:
         _call("gqt_vec_add", self.h, other.h)
@@ -439,13 +446,16 @@ def inner_product(state: Vector, left: Vector):
     return (re[0], im[0]) if state.nvec == 1 else (re, im)
 
 
-def moments(H: Hamiltonian, left: Vector, right: Vector, n_moments: int):
+def moments(H: Hamiltonian, left: Vector, right: Vector, n_moments: int,
+            precision: int | None = None):
     """mu_m = <left|T_m(H/E_max)|right>: shape (n_moments,), (nvec, n_moments), or for a
-    realisation batch (n_real, nvec, n_moments)."""
+    realisation batch (n_real, nvec, n_moments). `precision` runs the recurrence in
+    another arithmetic form than the vectors' (gqt_moments_form)."""
     R = getattr(H, "n_real", 1)
     re = np.zeros(n_moments * right.nvec * R)
     im = np.zeros(n_moments * right.nvec * R)
-    _call("gqt_moments", H.h, left.h, right.h, n_moments, _dptr(re), _dptr(im))
+    prec = right.precision if precision is None else precision
+    _call("gqt_moments_form", H.h, left.h, right.h, n_moments, prec, _dptr(re), _dptr(im))
     if R > 1:
         return re.reshape(R, right.nvec, n_moments), im.reshape(R, right.nvec, n_moments)
     if right.nvec > 1:

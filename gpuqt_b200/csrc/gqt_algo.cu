@@ -515,8 +515,81 @@ extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
   return GQT_OK;
 }
 
+static gqt_status convert_data(int n, int nvec, int from, const void* src, int to, void* dst)
+{
+  const size_t total = (size_t)n * nvec;
+  if (from == to) {
+    const size_t elem = from == GQT_FP64 ? sizeof(double2) : sizeof(float2);
+    if (src != dst)
+      GQT_CUDA(cudaMemcpyAsync(dst, src, total * elem, cudaMemcpyDeviceToDevice, stream()));
+    return GQT_OK;
+  }
+  const int grid = from == GQT_FP64 ? grid_for((const void*)k_convert<double2, float2>, total)
+                                    : grid_for((const void*)k_convert<float2, double2>, total);
+  if (from == GQT_FP64)
+    k_convert<double2, float2><<<grid, kBlock, 0, stream()>>>(total, (const double2*)src,
+                                                              (float2*)dst);
+  else
+    k_convert<float2, double2><<<grid, kBlock, 0, stream()>>>(total, (const float2*)src,
+                                                              (double2*)dst);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_vec_convert(gqt_vec* dst, const gqt_vec* src)
+{
+  if (!dst || !src || !dst->data || !src->data)
+    return fail(GQT_ERR_ARG, "gqt_vec_convert: null vector");
+  if (dst->n != src->n || dst->nvec != src->nvec)
+    return fail(GQT_ERR_ARG, "gqt_vec_convert: vectors differ in size or count");
+  return convert_data(src->n, src->nvec, src->precision, src->data, dst->precision, dst->data);
+}
+
+extern "C" gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
+                                              const gqt_vec* right, int M, int precision,
+                                              void* mu_dev)
+{
+  const char* w = "gqt_moments_device_form";
+  if (!h || !left || !right || !left->data || !right->data)
+    return fail(GQT_ERR_ARG, "%s: null argument", w);
+  if (precision == right->precision && precision == left->precision)
+    return gqt_moments_device(h, left, right, M, mu_dev);
+  if (!form_ops(precision, right->nvec))
+    return fail(GQT_ERR_ARG, "%s: form %d has no %d-vector launch", w, precision, right->nvec);
+  if (left->n != right->n || left->nvec != right->nvec)
+    return fail(GQT_ERR_ARG, "%s: left and right differ in size or count", w);
+  // The converted copies live in workspace slots 4 and 5 of the target form (slots
+  // 0-3 are the recurrence and evolution temporaries).
+  Workspace& ws = *h->ws;
+  const size_t bytes = (size_t)right->n * right->nvec *
+                       (precision == GQT_FP64 ? sizeof(double2) : sizeof(float2));
+  void *lc = nullptr, *rc = nullptr;
+  GQT_TRY(ws_vector(ws, precision, right->nvec, bytes, 5, &rc));
+  GQT_TRY(ws_vector(ws, precision, right->nvec, bytes, 4, &lc));
+  GQT_TRY(convert_data(right->n, right->nvec, right->precision, right->data, precision, rc));
+  const bool same = left->data == right->data;
+  if (!same)
+    GQT_TRY(convert_data(left->n, left->nvec, left->precision, left->data, precision, lc));
+  gqt_vec R = *right, L = *left;
+  R.precision = L.precision = precision;
+  R.bytes = L.bytes = bytes;
+  R.data = rc;
+  L.data = same ? rc : lc;
+  return gqt_moments_device(h, &L, &R, M, mu_dev);
+}
+
 extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
                                   int M, double* mu_re, double* mu_im)
+{
+  if (!right)
+    return fail(GQT_ERR_ARG, "gqt_moments: null vector");
+  return gqt_moments_form(h, left, right, M, right->precision, mu_re, mu_im);
+}
+
+extern "C" gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left,
+                                       const gqt_vec* right, int M, int precision,
+                                       double* mu_re, double* mu_im)
 {
   if (!mu_re || !mu_im)
     return fail(GQT_ERR_ARG, "gqt_moments: null output");
@@ -541,7 +614,7 @@ extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const g
       cudaGraphExecDestroy(kv.second);
     ws.graphs.clear();
   }
-  GQT_TRY(gqt_moments_device(h, left, right, M, ws.mu));
+  GQT_TRY(gqt_moments_device_form(h, left, right, M, precision, ws.mu));
   std::vector<double2> host((size_t)M * V);
   GQT_CUDA(cudaMemcpyAsync(host.data(), ws.mu, need, cudaMemcpyDeviceToHost, stream()));
   GQT_CUDA(cudaStreamSynchronize(stream()));

@@ -975,6 +975,16 @@ __global__ void __launch_bounds__(kBlock) k_segment_sum(const double2* __restric
   }
 }
 
+// dst = src across storage forms (FP64 <-> FP32).
+template <typename ST2, typename DT2>
+__global__ void __launch_bounds__(kBlock) k_convert(size_t total, const ST2* __restrict__ src,
+                                                    DT2* __restrict__ dst)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock)
+    st(dst + g, ld(src + g));
+}
+
 // FP64 accumulator -> FP32 state (end of an FP32-form evolution).
 template <typename OT2>
 __global__ void __launch_bounds__(kBlock) k_narrow(size_t total, const double2* __restrict__ in,

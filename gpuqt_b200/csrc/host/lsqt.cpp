@@ -167,9 +167,9 @@ extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
     return GQT_ERR_ARG;
   if (precision != GQT_FP64 && precision != GQT_FP32)
     return GQT_ERR_ARG;
-  const int saved = Vector::default_precision;
+  const int saved = Vector::moment_precision;
   gqt_host::ThrowScope scope;
-  Vector::default_precision = precision;
+  Vector::moment_precision = precision;
   gqt_status st = GQT_OK;
   try {
     Model model(dir, Model::Quiet{});
@@ -182,6 +182,6 @@ extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
     gqt_host::set_error(e.what());
     st = e.code;
   }
-  Vector::default_precision = saved;
+  Vector::moment_precision = saved;
   return st;
 }

@@ -19,7 +19,7 @@ int main(int argc, char* argv[])
   const char* driver = nullptr;
   for (int i = 1; i < argc; ++i) {
     if (std::strcmp(argv[i], "--fp32") == 0)
-      Vector::default_precision = GQT_FP32;
+      Vector::moment_precision = GQT_FP32;
     else if (!driver)
       driver = argv[i];
     else

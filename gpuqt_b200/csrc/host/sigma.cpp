@@ -18,10 +18,12 @@ using gqt_host::check;
 void find_moments_chebyshev(Model& model, Hamiltonian& H, Vector& state_left,
                             Vector& state_right, Vector& output)
 {
-  // One fused step+moment kernel per moment, replayed as a CUDA graph; the moments
-  // land in `output` (FP64, number_of_moments entries) on the device.
-  check(gqt_moments_device(H.handle(), state_left.handle(), state_right.handle(),
-                           model.number_of_moments, gqt_vec_data(output.handle())),
+  // One fused step+moment kernel per moment, replayed as a CUDA graph, in the form
+  // Vector::moment_precision; the moments land in `output` (FP64, number_of_moments
+  // entries) on the device.
+  check(gqt_moments_device_form(H.handle(), state_left.handle(), state_right.handle(),
+                                model.number_of_moments, Vector::moment_precision,
+                                gqt_vec_data(output.handle())),
         "find_moments_chebyshev");
 }
 

@@ -10,6 +10,7 @@
 using gqt_host::check;
 
 int Vector::default_precision = GQT_FP64;
+int Vector::moment_precision = GQT_FP64;
 
 Vector::Vector(int n_) : Vector(n_, default_precision) {}
 

@@ -39,14 +39,16 @@ def compare(g, model, mu64, mu32) -> dict:
 
 
 def vac_moments(g, model, H, phi, precision, steps):
-    left = g.Vector.from_host(*phi, precision=precision)
+    """VAC moment sets with FP64 states (evolved in FP64) and the recurrence in
+    `precision` (the library's FP32 form keeps the states FP64)."""
+    left = g.Vector.from_host(*phi)
     right = left.clone()
-    lcopy = g.Vector(model.n, precision=precision)
+    lcopy = g.Vector(model.n)
     g.apply_current(H, left, right)
     out = []
     for m in range(steps):
         g.apply_current(H, left, lcopy)
-        out.append(g.moments(H, right, lcopy, model.n_moments))
+        out.append(g.moments(H, right, lcopy, model.n_moments, precision=precision))
         if m < steps - 1:
             dt = model.time_step[m] * model.energy_max
             g.evolve(H, -1, dt, left)

@@ -57,30 +57,35 @@ class LibraryCompute:
         return self.g.chebyshev_summation(mu[0], mu[1], model.energy, model.energy_max,
                                           model.volume)
 
+    # States (and their time evolution) stay FP64; the moment recurrence runs in
+    # self.precision.
     def _vec(self, model, phi):
-        return self.g.Vector.from_host(*phi, precision=self.precision)
+        return self.g.Vector.from_host(*phi)
+
+    def _moments(self, H, left, right, model):
+        return self.g.moments(H, left, right, model.n_moments, precision=self.precision)
 
     def dos(self, model, H, phi):
         x = self._vec(model, phi)
-        return self._row(model, self.g.moments(H, x, x, model.n_moments))
+        return self._row(model, self._moments(H, x, x, model))
 
     def vac0(self, model, H, phi):
         g = self.g
         x = self._vec(model, phi)
-        v = g.Vector(model.n, precision=self.precision)
+        v = g.Vector(model.n)
         g.apply_current(H, x, v)
-        return self._row(model, g.moments(H, v, v, model.n_moments))
+        return self._row(model, self._moments(H, v, v, model))
 
     def vac(self, model, H, phi):
         g = self.g
         left = self._vec(model, phi)
         right = left.clone()
-        lcopy = g.Vector(model.n, precision=self.precision)
+        lcopy = g.Vector(model.n)
         g.apply_current(H, left, right)
         rows = []
         for m in range(model.n_steps):
             g.apply_current(H, left, lcopy)
-            rows.append(self._row(model, g.moments(H, right, lcopy, model.n_moments)))
+            rows.append(self._row(model, self._moments(H, right, lcopy, model)))
             if m < model.n_steps - 1:
                 dt = model.time_step[m] * model.energy_max
                 g.evolve(H, -1, dt, left)
@@ -91,13 +96,13 @@ class LibraryCompute:
         g = self.g
         state = self._vec(model, phi)
         sx = state.clone()
-        copy = g.Vector(model.n, precision=self.precision)
+        copy = g.Vector(model.n)
         dt = model.time_step[0] * model.energy_max
         g.evolve(H, 1, dt, state)
         g.evolvex(H, 1, dt, sx)
         rows = []
         for m in range(model.n_steps):
-            rows.append(self._row(model, g.moments(H, sx, sx, model.n_moments)))
+            rows.append(self._row(model, self._moments(H, sx, sx, model)))
             if m < model.n_steps - 1:
                 dt = model.time_step[m + 1] * model.energy_max
                 copy.copy_from(state)

@@ -192,6 +192,19 @@ gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* rig
  * [m][r][k], n_moments*count*nvec entries) and does not synchronise. */
 gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
                               int n_moments, void* mu_dev);
+/* As gqt_moments / gqt_moments_device, with the Chebyshev recurrence run in the
+ * arithmetic form `precision` whatever the form of left and right: FP64 states (for
+ * instance time-evolved ones, which keep their full precision across evolution
+ * steps) converted once into FP32 workspace vectors for the FP32-storage moment
+ * loop. With precision equal to the vectors' form this is gqt_moments. */
+gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                            int n_moments, int precision, double* mu_re, double* mu_im);
+gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
+                                   const gqt_vec* right, int n_moments, int precision,
+                                   void* mu_dev);
+/* dst = src across forms (FP64 <-> FP32, same sites and vector count); rounds to
+ * nearest when narrowing. */
+gqt_status gqt_vec_convert(gqt_vec* dst, const gqt_vec* src);
 /* Replaces evolve (src/sigma.cu:116-151): state <- U(direction * dt) state with
  * dt_scaled = dt * E_max. The Bessel coefficients J_m(dt_scaled) come from the host
  * libm (j0/j1/jn) and the series stops at the first m >= 2 with |J_m| < 1e-15, as
@@ -232,7 +245,8 @@ gqt_status gqt_model_time_step(const gqt_model* m, double* time_step);
 gqt_status gqt_model_initial_state(gqt_model* m, int orbital, double* re, double* im);
 /* Replaces lsqt(std::string) (src/lsqt.cu:135-152): the full run for one input
  * directory, appending dos.out / vac0.out / vac.out / msd.out / S.out / ldos.out
- * with the reference's formats. precision selects the arithmetic form. */
+ * with the reference's formats. precision selects the arithmetic form of the moment
+ * recurrence; states and their time evolution stay FP64. */
 gqt_status gqt_lsqt(const char* input_dir, int precision, int verbose);
 
 /* ---------------------------------------------------------------- no-allocation step */

@@ -31,6 +31,10 @@ public:
   int size() const { return n; }
   // Arithmetic form of vectors built with Vector(int); GQT_FP64 unless changed.
   static int default_precision;
+  // Arithmetic form of the Chebyshev recurrence in find_moments_chebyshev (GQT_FP32
+  // for the FP32-storage form); the states themselves keep default_precision, so
+  // time-evolved states stay FP64 across evolution steps.
+  static int moment_precision;
 
 private:
   gqt_vec* v = nullptr;

@@ -181,3 +181,35 @@ def test_fp32_evolution_close_to_fp64():
     ar, ai = a.download()
     br, bi = b.download()
     assert np.max(np.hypot(ar - br, ai - bi)) / np.max(np.hypot(ar, ai)) < 1e-6
+
+
+def test_moments_form_equals_fp32_vectors():
+    """FP64 states with the FP32 recurrence (gqt_moments_form) run exactly the
+    computation of FP32 vectors: the conversion rounds as the upload does."""
+    m, H, x64 = _setup("graphene_8x4")
+    re, im = x64.download()
+    x32 = g.Vector.from_host(re, im, precision=g.FP32)
+    a = g.moments(H, x64, x64, 300, precision=g.FP32)
+    b = g.moments(H, x32, x32, 300)
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    y = g.Vector(m.n)
+    g.apply_current(H, x64, y)
+    a = g.moments(H, y, x64, 300, precision=g.FP32)  # left != right
+    y32 = g.Vector(m.n, precision=g.FP32)
+    y32.convert_from(y)
+    b = g.moments(H, y32, x32, 300)
+    np.testing.assert_array_equal(a[0], b[0])
+
+
+def test_vec_convert_roundtrip():
+    rng = np.random.default_rng(4)
+    re, im = rng.normal(size=(4, 500)), rng.normal(size=(4, 500))
+    a = g.Vector.from_host(re, im, nvec=4)
+    b = g.Vector(500, nvec=4, precision=g.FP32)
+    b.convert_from(a)
+    r32, i32 = b.download()
+    np.testing.assert_array_equal(r32, re.astype(np.float32).astype(np.float64))
+    c = g.Vector(500, nvec=4)
+    c.convert_from(b)
+    np.testing.assert_array_equal(c.download()[1], im.astype(np.float32).astype(np.float64))
