@@ -37,18 +37,24 @@ sys.path.insert(0, ROOT)
 METRIC = "KPM site-moments/s + HBM GB/s: batched FP32/FP64-acc vs plain FP64 at ≤1e-6 err"
 UNIT = "site-moments/s"
 WORKLOAD = "graphene2m"
-# Algorithmic bytes per site-moment of the fused step (uniform rows, z = 3): ELL index
-# 4 B + complex hopping 16 B per neighbour, on-site potential 8 B, and four complex
-# vector streams (T_{m-2} read, T_{m-1} read once, T_m write, left read).
+# Algorithmic bytes per site-moment of the fused step (uniform rows, z = 3): per
+# neighbour entry 1 B in the coded format (a table row number; the table of distinct
+# (j - i, hopping, xx) entries sits in shared memory) or 20 B in the ELL format (index
+# 4 B + complex hopping 16 B); on-site potential 8 B; four complex vector streams
+# (T_{m-2} read, T_{m-1} read once, T_m write, left read).
 Z = 3
 
 
-def fp64_bytes_per_site(z=Z):
-    return z * (4 + 16) + 8 + 4 * 16
+def entry_bytes(coded):
+    return 1 if coded else 4 + 16
 
 
-def fp32_bytes_per_site_vector(V, z=Z):
-    return (z * (4 + 16) + 8) / V + 4 * 8
+def fp64_bytes_per_site(z=Z, coded=True):
+    return z * entry_bytes(coded) + 8 + 4 * 16
+
+
+def fp32_bytes_per_site_vector(V, z=Z, coded=True):
+    return (z * entry_bytes(coded) + 8) / V + 4 * 8
 
 
 def log(*a):
@@ -293,13 +299,15 @@ def run_ours(args):
         clocks = clk.summary()
         value = world * n * M * args.steps / (ms / 1e3)
         per_launch_s = t0.elapsed_time(t1) / 1e3 / (args.steps * M)
-        bpl = fp64_bytes_per_site() * n
+        coded = H.format == g.FORMAT_CODED
+        fmt = "coded" if coded else "ell"
+        bpl = fp64_bytes_per_site(coded=coded) * n
         achieved = bpl / per_launch_s / 1e9
         traffic = None
         tp = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tp):
             with open(tp) as f:
-                traffic = json.load(f).get("k_step_fp64_graphene2m_bytes_per_launch")
+                traffic = json.load(f).get(f"k_step_fp64_{fmt}_graphene2m_bytes_per_launch")
 
         # --- e2e: host phase vector (pinned) -> device, moments -> host, every step
         re_h = torch.from_numpy(np.ascontiguousarray(phi[0])).pin_memory()
@@ -349,12 +357,14 @@ def run_ours(args):
                 "config": {"workload": W.CONFIGS[WORKLOAD]["description"] +
                            "; one KPM moment set per step, one random-phase vector per GPU",
                            "form": "plain FP64 (reference arithmetic)",
+                           "operator_format": fmt + (f" ({H.n_codes} distinct entries)"
+                                                     if coded else ""),
                            "parallelism": f"replicas x{world}",
                            "l2": "inputs larger than L2 (220 MB touched per Chebyshev step)"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                              "unit": "GB/s", "frac": achieved / hbm_peak,
                              "traffic": traffic, "peak_kind": peak_kind,
-                             "kernel": "k_step<double2,V=1,Z=3,Exact,kCheb,dot>",
+                             "kernel": f"k_step<double2,V=1,Z=3,Exact,kCheb,dot> ({fmt})",
                              "bytes_per_launch": bpl},
                 "cpu_baseline": cpu,
                 "e2e": e2e,
@@ -382,6 +392,7 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
     x64 = g.Vector.from_host(*phi)
     r64, i64 = g.moments(H, x64, x64, M)
     fp64_rate = None
+    coded = H.format == g.FORMAT_CODED
     for V in (1, 16):
         vecs = [phi] + [m.initial_state() for _ in range(V - 1)]
         re = np.stack([v[0] for v in vecs])
@@ -399,26 +410,58 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         torch.cuda.synchronize()
         s = a.elapsed_time(b) / 1e3
         rate = V * n * M * reps / s
-        bpl = fp32_bytes_per_site_vector(V) * V * n
+        bpl = fp32_bytes_per_site_vector(V, coded=coded) * V * n
         ach = bpl / (s / (reps * M)) / 1e9
         r32, i32 = g.moments(H, X, X, M)
         r32, i32 = np.atleast_2d(r32)[0], np.atleast_2d(i32)[0]
         out[f"fp32_v{V}"] = {"site_moments_per_s": rate, "vectors_per_launch": V,
                              "achieved_gbs": ach, "frac": ach / hbm_peak,
-                             "bytes_per_site_moment": fp32_bytes_per_site_vector(V),
+                             "bytes_per_site_moment": fp32_bytes_per_site_vector(V, coded=coded),
                              "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32, i32))}
-    # FP64 rate from a short timed loop for the ratio
-    mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
-    a, b = ev()
-    a.record(stream)
-    for _ in range(3):
+        if V == 16 and coded:
+            # the same form on the plain ELL arrays
+            H.set_format(g.FORMAT_ELL)
+            g.moments_device(H, X, X, M, mu.data_ptr())
+            a, b = ev()
+            a.record(stream)
+            for _ in range(reps):
+                g.moments_device(H, X, X, M, mu.data_ptr())
+            b.record(stream)
+            torch.cuda.synchronize()
+            H.set_format(g.FORMAT_CODED)
+            s = a.elapsed_time(b) / 1e3
+            ach = fp32_bytes_per_site_vector(V, coded=False) * V * n / (s / (reps * M)) / 1e9
+            out["fp32_v16_ell"] = {"site_moments_per_s": V * n * M * reps / s,
+                                   "vectors_per_launch": V, "achieved_gbs": ach,
+                                   "frac": ach / hbm_peak,
+                                   "bytes_per_site_moment":
+                                       fp32_bytes_per_site_vector(V, coded=False)}
+
+    def fp64_rate(fmt):
+        # plain FP64 rate from a short timed loop, for the ratios
+        H.set_format(fmt)
+        mu = torch.empty(2 * M, dtype=torch.float64, device="cuda")
         g.moments_device(H, x64, x64, M, mu.data_ptr())
-    b.record(stream)
-    torch.cuda.synchronize()
-    fp64_rate = n * M * 3 / (a.elapsed_time(b) / 1e3)
-    for k in out:
-        out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / fp64_rate
-    out["fp64_v1_site_moments_per_s"] = fp64_rate
+        a, b = ev()
+        a.record(stream)
+        for _ in range(3):
+            g.moments_device(H, x64, x64, M, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        return n * M * 3 / (a.elapsed_time(b) / 1e3)
+
+    default = H.format
+    rate64 = fp64_rate(default)
+    rate64_ell = fp64_rate(g.FORMAT_ELL) if coded else rate64
+    H.set_format(default)
+    for k in [k for k in out if k.startswith("fp32")]:
+        out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / rate64
+        out[k]["speedup_vs_fp64_ell"] = out[k]["site_moments_per_s"] / rate64_ell
+    out["fp64_v1_site_moments_per_s"] = rate64
+    ach = fp64_bytes_per_site(coded=False) * rate64_ell / 1e9
+    out["fp64_v1_ell"] = {"site_moments_per_s": rate64_ell, "achieved_gbs": ach,
+                          "frac": ach / hbm_peak,
+                          "bytes_per_site_moment": fp64_bytes_per_site(coded=False)}
     # Bessel evolution of one MSD step (1 fs): evolve and evolvex, FP64.
     dt = m.time_step[0] * m.energy_max
     st = x64.clone()
@@ -479,7 +522,8 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
         torch.cuda.synchronize()
         total_ms += a.elapsed_time(b)
     rate = vectors * sites * moments / (total_ms / 1e3)
-    bytes_site_moment = fp32_bytes_per_site_vector(V, z=4) * B.n / sites
+    bytes_site_moment = (fp32_bytes_per_site_vector(V, z=4, coded=B.format == g.FORMAT_CODED)
+                         * B.n / sites)
     # DOS error of vector 0 of realisation 0 against its FP64 moments
     X.upload(*B.scatter(per0))
     r32, i32 = g.moments(B, X, X, moments)
@@ -490,6 +534,7 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
     err = dos_error(g, m0, (r64, i64), (r32[0, 0], i32[0, 0]))
     return {"realisations": [[m.n, round(m.energy_max, 4)] for m in models],
             "sites": sites, "padded_sites": B.n, "vectors": vectors, "moments": moments,
+            "operator_format": "coded" if B.format == g.FORMAT_CODED else "ell",
             "autotuned_vectors_per_launch": V, "autotune_rates": rates,
             "site_moments_per_s": rate, "ms_total": total_ms,
             "achieved_gbs": rate * bytes_site_moment / 1e9,

@@ -25,6 +25,8 @@ CLI_PATH = os.path.join(HERE, "lib", "lsqt_b200")
 
 FP64 = 0
 FP32 = 1
+FORMAT_ELL = 0    # the reference's ELL arrays
+FORMAT_CODED = 1  # one byte per ELL entry into a table of the distinct entries
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -63,6 +65,8 @@ _SIGS = {
     "gqt_ham_create": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.POINTER(_vp)]),
     "gqt_ham_destroy": (ctypes.c_int, [_vp]),
     "gqt_ham_info": (ctypes.c_int, [_vp, _ip, _ip, _ip, _dp]),
+    "gqt_ham_set_format": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gqt_ham_format": (ctypes.c_int, [_vp, _ip, _ip]),
     "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
                                             ctypes.POINTER(_vp)]),
     "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
@@ -349,6 +353,22 @@ class Hamiltonian:
             _call("gqt_ham_realisation", self.h, k, ctypes.byref(off), ctypes.byref(nr),
                   ctypes.byref(em))
             self.realisations.append((off.value, nr.value, em.value))
+
+    @property
+    def format(self) -> int:
+        f = ctypes.c_int()
+        _call("gqt_ham_format", self.h, ctypes.byref(f), None)
+        return f.value
+
+    @property
+    def n_codes(self) -> int:
+        c = ctypes.c_int()
+        _call("gqt_ham_format", self.h, None, ctypes.byref(c))
+        return c.value
+
+    def set_format(self, fmt: int) -> None:
+        """FORMAT_ELL or FORMAT_CODED (the default when the operator has a coded form)."""
+        _call("gqt_ham_set_format", self.h, fmt)
 
     @classmethod
     def batch(cls, models) -> "Hamiltonian":

@@ -78,7 +78,14 @@ namespace {
 
 Op make_op(const gqt_ham* h, int nvec = 1)
 {
-  Op op;
+  Op op{};
+  if (h->use_codes) {
+    op.code = h->code;
+    op.code_delta = h->code_delta;
+    op.code_hop = h->code_hop;
+    op.code_xx = h->code_xx;
+    op.n_codes = h->n_codes;
+  }
   op.wpt = (nvec >= 0 && nvec <= 32) ? h->wpt[nvec] : 0;
   op.n = h->n;
   op.z = h->z;
@@ -90,6 +97,7 @@ Op make_op(const gqt_ham* h, int nvec = 1)
   op.xx = h->xx;
   op.emax = h->energy_max;
   op.inv_emax = 1.0 / h->energy_max;
+  op.lib_div = !(h->energy_max >= 0x1p-100 && h->energy_max <= 0x1p100);
   return op;
 }
 

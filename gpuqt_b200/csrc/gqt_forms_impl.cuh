@@ -33,6 +33,18 @@ gqt_status launch(K* kernel, size_t total, Args... args)
   return GQT_OK;
 }
 
+// Kernels that read the operator take Op first; with a coded operator its table
+// goes to dynamic shared memory.
+template <typename K, typename... Args>
+gqt_status launch_op(K* kernel, size_t total, const Op& op, Args... args)
+{
+  const int grid = grid_for((const void*)kernel, total);
+  kernel<<<grid, kBlock, op_smem_bytes(op), stream()>>>(op, args...);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
 template <typename K, typename... Args>
 gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
 {
@@ -76,14 +88,14 @@ struct FormImpl {
           const size_t items = (size_t)op.n * (V / WW);
           if (mode == kApply) {
             if (dot)
-              return launch(k_step_vec<VT2, V, WW, Z, A, kApply, true>, items, op, a0, a1, o, l,
+              return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, true>, items, op, a0, a1, o, l,
                             d);
-            return launch(k_step_vec<VT2, V, WW, Z, A, kApply, false>, items, op, a0, a1, o, l,
+            return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, false>, items, op, a0, a1, o, l,
                           d);
           }
           if (dot)
-            return launch(k_step_vec<VT2, V, WW, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
-          return launch(k_step_vec<VT2, V, WW, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
+            return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
+          return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
         };
         if constexpr (W2 != W) {
           if (op.wpt == W2)
@@ -93,12 +105,12 @@ struct FormImpl {
       }
       if (mode == kApply) {
         if (dot)
-          return launch(k_step<VT2, V, Z, A, kApply, true>, total, op, a0, a1, o, l, d);
-        return launch(k_step<VT2, V, Z, A, kApply, false>, total, op, a0, a1, o, l, d);
+          return launch_op(k_step<VT2, V, Z, A, kApply, true>, total, op, a0, a1, o, l, d);
+        return launch_op(k_step<VT2, V, Z, A, kApply, false>, total, op, a0, a1, o, l, d);
       }
       if (dot)
-        return launch(k_step<VT2, V, Z, A, kCheb, true>, total, op, a0, a1, o, l, d);
-      return launch(k_step<VT2, V, Z, A, kCheb, false>, total, op, a0, a1, o, l, d);
+        return launch_op(k_step<VT2, V, Z, A, kCheb, true>, total, op, a0, a1, o, l, d);
+      return launch_op(k_step<VT2, V, Z, A, kCheb, false>, total, op, a0, a1, o, l, d);
     });
   }
 
@@ -115,7 +127,7 @@ struct FormImpl {
       constexpr int Z = decltype(zc)::value;
       auto go = [&](auto* kernel) -> gqt_status {
         md.blocks = grid_for((const void*)kernel, items);
-        kernel<<<md.blocks, kBlock, 0, stream()>>>(op, a0, a1, o, l, md);
+        kernel<<<md.blocks, kBlock, op_smem_bytes(op), stream()>>>(op, a0, a1, o, l, md);
         count_launches(1);
         GQT_CUDA(cudaGetLastError());
         return GQT_OK;
@@ -151,8 +163,8 @@ struct FormImpl {
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
       if (current)
-        return launch(k_xop<VT2, V, Z, A, true>, total, op, (const VT2*)in, (VT2*)out);
-      return launch(k_xop<VT2, V, Z, A, false>, total, op, (const VT2*)in, (VT2*)out);
+        return launch_op(k_xop<VT2, V, Z, A, true>, total, op, (const VT2*)in, (VT2*)out);
+      return launch_op(k_xop<VT2, V, Z, A, false>, total, op, (const VT2*)in, (VT2*)out);
     });
   }
 
@@ -169,7 +181,7 @@ struct FormImpl {
     const size_t total = (size_t)op.n * V;
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
-      return launch(k_cheb2<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+      return launch_op(k_cheb2<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
                     (const VT2*)s1, (VT2*)s2, out, bessel, label);
     });
   }
@@ -186,7 +198,7 @@ struct FormImpl {
     const size_t total = (size_t)op.n * V;
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
-      return launch(k_cheb2x<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+      return launch_op(k_cheb2x<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
                     (const VT2*)s0x, (const VT2*)s1, (const VT2*)s1x, (VT2*)s2, (VT2*)s2x,
                     out, bessel, label);
     });

@@ -74,6 +74,15 @@ struct gqt_ham {
   double* xx = nullptr;     // [z*n] column-major
   double* pot = nullptr;    // [n]
   bool has_xx = false;
+  // Coded operator (built when the (j - i, hopping, xx) entries of the ELL take at
+  // most GQT_MAX_CODES distinct values, as lattice models do): one byte per entry and
+  // a small table holding the same doubles, so results are unchanged.
+  uint8_t* code = nullptr;      // [z*n] column-major
+  int* code_delta = nullptr;    // [n_codes]: j - i
+  double2* code_hop = nullptr;  // [n_codes]
+  double* code_xx = nullptr;    // [n_codes]
+  int n_codes = 0;
+  int use_codes = 0;            // kernels read the codes (default when they exist)
   // Realisation batch (gqt_ham_create_batch): n_real > 1 block-diagonal models, each
   // padded to whole tiles and pre-divided by its own E_max (energy_max is then 1).
   int n_real = 1;

@@ -40,8 +40,16 @@ struct Op {
   const double* __restrict__ pot;
   const double* __restrict__ xx;
   double emax;
-  double inv_emax;
+  double inv_emax;  // RN(1 / emax)
+  int lib_div;      // 1: emax outside [2^-100, 2^100], divide with __ddiv_rn
   int wpt;  // vectors per thread chosen for this launch (0: the form's default)
+  // Coded operator (null code: read the ELL arrays above): entry e is row code[e] of
+  // the table, giving j - i, the hopping and xx.
+  const uint8_t* __restrict__ code;
+  const int* __restrict__ code_delta;
+  const double2* __restrict__ code_hop;
+  const double* __restrict__ code_xx;
+  int n_codes;
 };
 
 struct Dot {
@@ -50,14 +58,81 @@ struct Dot {
   double2* mu;       // this moment's V results
 };
 
+// ------------------------------------------------------------------ operator entries
+// The coded operator's table, staged in dynamic shared memory at kernel start
+// (n_codes * 28 bytes, passed at launch as op_smem_bytes). `op.code` is the same for
+// every thread, so the branches below never diverge.
+struct Tables {
+  const int* delta;
+  const double2* hop;
+  const double* xx;
+};
+
+inline size_t op_smem_bytes(const Op& op) { return op.code ? (size_t)op.n_codes * 28 : 0; }
+
+__device__ __forceinline__ Tables load_tables(const Op& op)
+{
+  extern __shared__ __align__(16) unsigned char dyn_smem[];
+  if (!op.code)
+    return Tables{nullptr, nullptr, nullptr};
+  const int n = op.n_codes;
+  double2* hop = reinterpret_cast<double2*>(dyn_smem);
+  double* xx = reinterpret_cast<double*>(dyn_smem + (size_t)n * 16);
+  int* delta = reinterpret_cast<int*>(dyn_smem + (size_t)n * 24);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    hop[k] = op.code_hop[k];
+    xx[k] = op.code_xx[k];
+    delta[k] = op.code_delta[k];
+  }
+  __syncthreads();
+  return Tables{delta, hop, xx};
+}
+
+// Entry e = m * n + i of row i: neighbour j, hopping h, and the table row c (coded
+// form only) for ell_xx.
+__device__ __forceinline__ void ell_entry(const Op& op, const Tables& tb, size_t e, int i,
+                                          int& j, double2& h, int& c)
+{
+  if (tb.hop) {
+    c = op.code[e];
+    j = i + tb.delta[c];
+    h = tb.hop[c];
+  } else {
+    c = 0;
+    j = op.nl[e];
+    h = op.hop[e];
+  }
+}
+
+__device__ __forceinline__ double ell_xx(const Op& op, const Tables& tb, size_t e, int c)
+{
+  return tb.hop ? tb.xx[c] : op.xx[e];
+}
+
 // ------------------------------------------------------------------ arithmetic
 struct ExactArith {
   static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
   static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
   static __device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+  // a / E_max correctly rounded, from fused multiply-adds (Markstein's theorem:
+  // P. W. Markstein, IBM J. Res. Dev. 34(1), 1990; Muller et al., Handbook of
+  // Floating-Point Arithmetic, FMA-based division). With y = RN(1/E) (op.inv_emax, an
+  // IEEE division on the host) and q within one ulp of a/E, r = a - qE is exact and
+  // RN(q + r y) = RN(a/E). q0 = RN(a y) is within 1.5 ulp; one correction makes it
+  // faithful, the second rounds correctly. The exact remainders need |a| and E well
+  // inside the normal range: zero, tiny, huge or non-finite a, and an E outside
+  // [2^-100, 2^100] (op.lib_div), take the library division.
   static __device__ __forceinline__ double scale(double a, const Op& op)
   {
-    return __ddiv_rn(a, op.emax);
+    const double m = fabs(a);
+    if (!(m >= 0x1p-900 && m <= 0x1p900) || op.lib_div)
+      return __ddiv_rn(a, op.emax);
+    const double b = op.emax, y = op.inv_emax;
+    double q = __dmul_rn(a, y);
+    double r = __fma_rn(-q, b, a);
+    q = __fma_rn(r, y, q);
+    r = __fma_rn(-q, b, a);
+    return __fma_rn(r, y, q);
   }
   // a*c - b*d and a*d + b*c, each product and sum rounded on its own
   static __device__ __forceinline__ double cre(double a, double b, double c, double d)
@@ -320,8 +395,8 @@ __device__ __forceinline__ void stw(double2* p, const double2 (&v)[W])
 // acc += sum_m H_im x_{j_m} for one (site i, vector v), neighbours in ELL order.
 // Z > 0: the row length bound is known at compile time and the loop is unrolled.
 template <int V, int Z, class A, typename VT2>
-__device__ __forceinline__ void hop_row(const Op& op, int i, int v, const VT2* __restrict__ x,
-                                        double& tr, double& ti)
+__device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, int v,
+                                        const VT2* __restrict__ x, double& tr, double& ti)
 {
   const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
   if constexpr (Z > 0) {
@@ -329,8 +404,9 @@ __device__ __forceinline__ void hop_row(const Op& op, int i, int v, const VT2* _
     for (int m = 0; m < Z; ++m) {
       if (m < cnt) {
         const size_t e = (size_t)m * op.n + i;
-        const int j = op.nl[e];
-        const double2 h = op.hop[e];
+        int j, c;
+        double2 h;
+        ell_entry(op, tb, e, i, j, h, c);
         const double2 y = ld(x + (size_t)j * V + v);
         tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
         ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
@@ -339,8 +415,9 @@ __device__ __forceinline__ void hop_row(const Op& op, int i, int v, const VT2* _
   } else {
     for (int m = 0; m < cnt; ++m) {
       const size_t e = (size_t)m * op.n + i;
-      const int j = op.nl[e];
-      const double2 h = op.hop[e];
+      int j, c;
+      double2 h;
+      ell_entry(op, tb, e, i, j, h, c);
       const double2 y = ld(x + (size_t)j * V + v);
       tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
       ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
@@ -350,37 +427,224 @@ __device__ __forceinline__ void hop_row(const Op& op, int i, int v, const VT2* _
 
 enum StepMode { kApply = 0, kCheb = 1 };
 
+#ifndef GQT_STEP_PREFETCH
+#define GQT_STEP_PREFETCH 2
+#endif
+
+// One site's row, fetched one grid-stride iteration ahead of its use: the row length
+// and the table rows (coded form) or neighbour indices (ELL form) of its Z entries.
+// Entries past the row length are in bounds (padding) and skipped through cnt.
+template <int Z>
+struct RowIdx {
+  int cnt;
+  int idx[Z];
+};
+
+template <int Z>
+__device__ __forceinline__ void fetch_row(const Op& op, const Tables& tb, int i, RowIdx<Z>& r)
+{
+  r.cnt = op.uniform ? Z : op.nn[i];
+#pragma unroll
+  for (int m = 0; m < Z; ++m) {
+    const size_t e = (size_t)m * op.n + i;
+    r.idx[m] = tb.hop ? (int)op.code[e] : op.nl[e];
+  }
+}
+
+// hop_row from a prefetched row: every gather is issued before the arithmetic, which
+// keeps the reference's neighbour order.
+template <int V, int Z, class A, typename VT2>
+__device__ __forceinline__ void hop_row_pre(const Op& op, const Tables& tb, int i, int v,
+                                            const RowIdx<Z>& r, const VT2* __restrict__ x,
+                                            double& tr, double& ti)
+{
+  int j[Z];
+  double2 h[Z], y[Z];
+#pragma unroll
+  for (int m = 0; m < Z; ++m) {
+    if (tb.hop) {
+      j[m] = i + tb.delta[r.idx[m]];
+      h[m] = tb.hop[r.idx[m]];
+    } else {
+      j[m] = r.idx[m];
+      h[m] = m < r.cnt ? op.hop[(size_t)m * op.n + i] : make_double2(0.0, 0.0);
+    }
+  }
+#pragma unroll
+  for (int m = 0; m < Z; ++m)
+    if (m < r.cnt)
+      y[m] = ld(x + (size_t)j[m] * V + v);
+#pragma unroll
+  for (int m = 0; m < Z; ++m) {
+    if (m < r.cnt) {
+      tr = A::add(tr, A::cre(h[m].x, h[m].y, y[m].x, y[m].y));
+      ti = A::add(ti, A::cim(h[m].x, h[m].y, y[m].x, y[m].y));
+    }
+  }
+}
+
+// Neighbour j and hopping h of entry m of row i, from its prefetched index.
+__device__ __forceinline__ void row_entry(const Op& op, const Tables& tb, int i, int m,
+                                          int idx, int& j, double2& h)
+{
+  if (tb.hop) {
+    j = i + tb.delta[idx];
+    h = tb.hop[idx];
+  } else {
+    j = idx;
+    h = op.hop[(size_t)m * op.n + i];
+  }
+}
+
+// acc[k] += sum_m H_im x_{j_m, v0 + k} for W consecutive vectors, from a prefetched row.
+template <int V, int W, int Z, class A, typename VT2>
+__device__ __forceinline__ void hop_row_w(const Op& op, const Tables& tb, int i, int v0,
+                                          const RowIdx<Z>& r, const VT2* __restrict__ x,
+                                          double (&tr)[W], double (&ti)[W])
+{
+#pragma unroll
+  for (int m = 0; m < Z; ++m) {
+    if (m < r.cnt) {
+      int j;
+      double2 h;
+      row_entry(op, tb, i, m, r.idx[m], j, h);
+      double2 y[W];
+      ldw<W>(x + (size_t)j * V + v0, y);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+        ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+      }
+    }
+  }
+}
+
+// xx of entry m of row i, from its prefetched index.
+__device__ __forceinline__ double row_xx(const Op& op, const Tables& tb, int i, int m, int idx)
+{
+  return tb.hop ? tb.xx[idx] : op.xx[(size_t)m * op.n + i];
+}
+
+// Runs f(g, row) over this thread's grid-stride items g < total (site g / PER), with
+// each item's row loaded one iteration ahead: an iteration then waits on one memory
+// round trip (its gathers) instead of two (row, then gathers).
+template <int Z, int PER, class F>
+__device__ __forceinline__ void pipelined_rows(const Op& op, const Tables& tb, size_t total,
+                                               F&& f)
+{
+  const size_t stride = (size_t)gridDim.x * kBlock;
+  size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
+  RowIdx<Z> cur;
+  if (g < total)
+    fetch_row<Z>(op, tb, (int)(g / PER), cur);
+  for (; g < total; g += stride) {
+    RowIdx<Z> nxt = cur;
+    if (g + stride < total)
+      fetch_row<Z>(op, tb, (int)((g + stride) / PER), nxt);
+    f(g, cur);
+    cur = nxt;
+  }
+}
+
+// The streamed inputs of one element: potential, T_{m-1}, T_{m-2} and left.
+struct Streams {
+  double p;
+  double2 x, y0, l;
+};
+
+template <typename VT2, int V, int MODE, bool DOT>
+__device__ __forceinline__ void fetch_streams(const Op& op, size_t g, const VT2* t0,
+                                              const VT2* __restrict__ t1,
+                                              const VT2* __restrict__ left, Streams& s)
+{
+  s.p = op.pot[g / V];
+  s.x = ld(t1 + g);
+  s.y0 = make_double2(0.0, 0.0);
+  s.l = s.y0;
+  if constexpr (MODE == kCheb)
+    s.y0 = ld(t0 + g);
+  if constexpr (DOT)
+    s.l = ld(left + g);
+}
+
 // out = H t1 / E_max (kApply) or out = 2 H t1 / E_max - t0 (kCheb), optionally fused
 // with the moment <left|out>. out may alias t0 (a site reads t0 before writing out).
 // Follows gpu_apply_hamiltonian / gpu_kernel_polynomial (src/hamiltonian.cu:153-186,
 // :886-925) with gpu_find_inner_product_1/2 (src/vector.cu:243-401) fused in.
+//
+// With a compile-time row bound (Z > 0) the grid-stride loop is software-pipelined:
+// the next element's row indices are loaded while this element's gathers are in
+// flight, so an iteration waits on one memory round trip (the gathers) instead of
+// two (row, then gathers).
 template <typename VT2, int V, int Z, class A, int MODE, bool DOT>
 __global__ void __launch_bounds__(kBlock) k_step(Op op, const VT2* t0,
                                                  const VT2* __restrict__ t1, VT2* out,
                                                  const VT2* __restrict__ left, Dot dot)
 {
+  const Tables tb = load_tables(op);
   const size_t total = (size_t)op.n * V;
+  const size_t stride = (size_t)gridDim.x * kBlock;
   CSum re{0.0, 0.0}, im{0.0, 0.0};
-  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
-       g += (size_t)gridDim.x * kBlock) {
-    const int i = (int)(g / V);
-    const int v = (int)(g % V);
-    const double p = op.pot[i];
-    const double2 x = ld(t1 + g);
-    double tr = A::mul(p, x.x);
-    double ti = A::mul(p, x.y);
-    hop_row<V, Z, A>(op, i, v, t1, tr, ti);
-    tr = A::scale(tr, op);
-    ti = A::scale(ti, op);
-    if constexpr (MODE == kCheb) {
-      const double2 y0 = ld(t0 + g);
-      tr = A::two_x_minus(tr, y0.x);
-      ti = A::two_x_minus(ti, y0.y);
+  size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
+  if constexpr (Z > 0 && GQT_STEP_PREFETCH > 0) {
+    RowIdx<Z> cur;
+    Streams sc;
+    if (g < total) {
+      fetch_row<Z>(op, tb, (int)(g / V), cur);
+      if constexpr (GQT_STEP_PREFETCH > 1)
+        fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, sc);
     }
-    const double2 r = make_double2(tr, ti);
-    st(out + g, r);
-    if constexpr (DOT)
-      dot_term(re, im, stored(out, r), ld(left + g));
+    for (; g < total; g += stride) {
+      const int i = (int)(g / V);
+      const int v = (int)(g % V);
+      const size_t gn = g + stride;
+      Streams s;
+      if constexpr (GQT_STEP_PREFETCH > 1)
+        s = sc;
+      else
+        fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, s);
+      RowIdx<Z> nxt = cur;
+      if (gn < total) {
+        fetch_row<Z>(op, tb, (int)(gn / V), nxt);
+        if constexpr (GQT_STEP_PREFETCH > 1)
+          fetch_streams<VT2, V, MODE, DOT>(op, gn, t0, t1, left, sc);
+      }
+      double tr = A::mul(s.p, s.x.x);
+      double ti = A::mul(s.p, s.x.y);
+      hop_row_pre<V, Z, A>(op, tb, i, v, cur, t1, tr, ti);
+      tr = A::scale(tr, op);
+      ti = A::scale(ti, op);
+      if constexpr (MODE == kCheb) {
+        tr = A::two_x_minus(tr, s.y0.x);
+        ti = A::two_x_minus(ti, s.y0.y);
+      }
+      const double2 r = make_double2(tr, ti);
+      st(out + g, r);
+      if constexpr (DOT)
+        dot_term(re, im, stored(out, r), s.l);
+      cur = nxt;
+    }
+  } else {
+    for (; g < total; g += stride) {
+      const int i = (int)(g / V);
+      const int v = (int)(g % V);
+      const double p = op.pot[i];
+      const double2 x = ld(t1 + g);
+      double tr = A::mul(p, x.x);
+      double ti = A::mul(p, x.y);
+      hop_row<V, Z, A>(op, tb, i, v, t1, tr, ti);
+      tr = A::scale(tr, op);
+      ti = A::scale(ti, op);
+      if constexpr (MODE == kCheb) {
+        const double2 y0 = ld(t0 + g);
+        tr = A::two_x_minus(tr, y0.x);
+        ti = A::two_x_minus(ti, y0.y);
+      }
+      const double2 r = make_double2(tr, ti);
+      st(out + g, r);
+      if constexpr (DOT)
+        dot_term(re, im, stored(out, r), ld(left + g));
+    }
   }
   if constexpr (DOT)
     dot_finish<V>(re, im, dot);
@@ -408,6 +672,7 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
                                                      const VT2* __restrict__ t1, VT2* out,
                                                      const VT2* __restrict__ left, Dot dot)
 {
+  const Tables tb = load_tables(op);
   constexpr int kTps = V / W;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
   const size_t items = (size_t)op.n * kTps;
@@ -415,8 +680,8 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
 #pragma unroll
   for (int k = 0; k < W; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
-  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < items;
-       g += (size_t)gridDim.x * kBlock) {
+  // One item: W consecutive vectors of one site; `row` adds the neighbour terms.
+  auto item = [&](size_t g, auto&& row) {
     const int i = (int)(g / kTps);
     const int v0 = (int)(g % kTps) * W;
     const size_t base = (size_t)i * V + v0;
@@ -429,28 +694,7 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
       tr[k] = A::mul(p, x[k].x);
       ti[k] = A::mul(p, x[k].y);
     }
-    const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
-    auto body = [&](int m) {
-      const size_t e = (size_t)m * op.n + i;
-      const int j = op.nl[e];
-      const double2 h = op.hop[e];
-      double2 y[W];
-      ldw<W>(t1 + (size_t)j * V + v0, y);
-#pragma unroll
-      for (int k = 0; k < W; ++k) {
-        tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
-        ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
-      }
-    };
-    if constexpr (Z > 0) {
-#pragma unroll
-      for (int m = 0; m < Z; ++m)
-        if (m < cnt)
-          body(m);
-    } else {
-      for (int m = 0; m < cnt; ++m)
-        body(m);
-    }
+    row(i, v0, tr, ti);
     double2 r[W];
     if constexpr (MODE == kCheb) {
       double2 y0[W];
@@ -477,6 +721,42 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
           im[k].s = fma(r[k].y, l[k].x, fma(-r[k].x, l[k].y, im[k].s));
         }
       }
+    }
+  };
+  const size_t stride = (size_t)gridDim.x * kBlock;
+  size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
+  if constexpr (Z > 0 && GQT_STEP_PREFETCH > 0) {
+    // Software-pipelined as in k_step: the next item's row is loaded first.
+    RowIdx<Z> cur;
+    if (g < items)
+      fetch_row<Z>(op, tb, (int)(g / kTps), cur);
+    for (; g < items; g += stride) {
+      RowIdx<Z> nxt = cur;
+      if (g + stride < items)
+        fetch_row<Z>(op, tb, (int)((g + stride) / kTps), nxt);
+      item(g, [&](int i, int v0, double(&tr)[W], double(&ti)[W]) {
+        hop_row_w<V, W, Z, A>(op, tb, i, v0, cur, t1, tr, ti);
+      });
+      cur = nxt;
+    }
+  } else {
+    for (; g < items; g += stride) {
+      item(g, [&](int i, int v0, double(&tr)[W], double(&ti)[W]) {
+        const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+        for (int m = 0; m < cnt; ++m) {
+          const size_t e = (size_t)m * op.n + i;
+          int j, c;
+          double2 h;
+          ell_entry(op, tb, e, i, j, h, c);
+          double2 y[W];
+          ldw<W>(t1 + (size_t)j * V + v0, y);
+#pragma unroll
+          for (int k = 0; k < W; ++k) {
+            tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+            ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+          }
+        }
+      });
     }
   }
   if constexpr (DOT)
@@ -551,6 +831,7 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
                                                        const VT2* __restrict__ left, MultiDot md)
 {
+  const Tables tb = load_tables(op);
   constexpr int kTps = V / W;
   constexpr int kWarps = kBlock / 32;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
@@ -590,8 +871,20 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
         ++r;
     }
     any = true;
+    // Software-pipelined within the tile: the next item's row is loaded first.
+    constexpr bool kPre = Z > 0 && GQT_STEP_PREFETCH > 0 && MODE != kDotOnly;
+    RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
+    if constexpr (kPre) {
+      if (threadIdx.x < items_per_tile)
+        fetch_row(op, tb, (int)(((size_t)t * items_per_tile + threadIdx.x) / kTps), cur);
+    }
     for (size_t it = threadIdx.x; it < items_per_tile; it += kBlock) {
       const size_t g = (size_t)t * items_per_tile + it;
+      if constexpr (kPre) {
+        nxt = cur;
+        if (it + kBlock < items_per_tile)
+          fetch_row(op, tb, (int)((g + kBlock) / kTps), nxt);
+      }
       const int i = (int)(g / kTps);
       const int v0 = (int)(g % kTps) * W;
       const size_t base = (size_t)i * V + v0;
@@ -608,27 +901,23 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
           tr[k] = A::mul(p, x[k].x);
           ti[k] = A::mul(p, x[k].y);
         }
-        const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
-        auto body = [&](int m) {
-          const size_t e = (size_t)m * op.n + i;
-          const int j = op.nl[e];
-          const double2 h = op.hop[e];
-          double2 y[W];
-          ldw<W>(t1 + (size_t)j * V + v0, y);
-#pragma unroll
-          for (int k = 0; k < W; ++k) {
-            tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
-            ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
-          }
-        };
-        if constexpr (Z > 0) {
-#pragma unroll
-          for (int m = 0; m < Z; ++m)
-            if (m < cnt)
-              body(m);
+        if constexpr (kPre) {
+          hop_row_w<V, W, (Z > 0 ? Z : 1), A>(op, tb, i, v0, cur, t1, tr, ti);
         } else {
-          for (int m = 0; m < cnt; ++m)
-            body(m);
+          const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+          for (int m = 0; m < cnt; ++m) {
+            const size_t e = (size_t)m * op.n + i;
+            int j, c;
+            double2 h;
+            ell_entry(op, tb, e, i, j, h, c);
+            double2 y[W];
+            ldw<W>(t1 + (size_t)j * V + v0, y);
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+              tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+              ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+            }
+          }
         }
         if constexpr (MODE == kCheb) {
           double2 y0[W];
@@ -655,6 +944,8 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
           im[k].s = fma(r2[k].y, l[k].x, fma(-r2[k].x, l[k].y, im[k].s));
         }
       }
+      if constexpr (kPre)
+        cur = nxt;
     }
   }
   if (any)
@@ -710,40 +1001,55 @@ template <typename VT2, int V, int Z, class A, bool CURRENT>
 __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ in,
                                                 VT2* __restrict__ out)
 {
+  const Tables tb = load_tables(op);
   const size_t total = (size_t)op.n * V;
-  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
-       g += (size_t)gridDim.x * kBlock) {
-    const int i = (int)(g / V);
-    const int v = (int)(g % V);
-    const int cnt = op.uniform ? op.z : op.nn[i];
-    double tr = 0.0, ti = 0.0;
-    auto body = [&](int m) {
-      const size_t e = (size_t)m * op.n + i;
-      const int j = op.nl[e];
-      const double2 h = op.hop[e];
-      const double2 y = ld(in + (size_t)j * V + v);
-      const double x = op.xx[e];
-      if constexpr (CURRENT) {
-        tr = A::add(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
-        ti = A::add(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
-      } else {
-        tr = A::sub(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
-        ti = A::sub(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
-      }
-    };
-    if constexpr (Z > 0) {
-#pragma unroll
-      for (int m = 0; m < Z; ++m)
-        if (m < cnt)
-          body(m);
+  auto term = [&](double& tr, double& ti, double2 h, double2 y, double x) {
+    if constexpr (CURRENT) {
+      tr = A::add(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
+      ti = A::add(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
     } else {
-      for (int m = 0; m < cnt; ++m)
-        body(m);
+      tr = A::sub(tr, A::mul(A::cre(h.x, h.y, y.x, y.y), x));
+      ti = A::sub(ti, A::mul(A::cim(h.x, h.y, y.x, y.y), x));
     }
+  };
+  auto finish = [&](size_t g, double tr, double ti) {
     if constexpr (CURRENT) {
       st(out + g, make_double2(ti, -tr));
     } else {
       st(out + g, make_double2(A::scale(tr, op), A::scale(ti, op)));
+    }
+  };
+  if constexpr (Z > 0) {
+    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+      const int i = (int)(g / V);
+      const int v = (int)(g % V);
+      double tr = 0.0, ti = 0.0;
+#pragma unroll
+      for (int m = 0; m < Z; ++m) {
+        if (m < r.cnt) {
+          int j;
+          double2 h;
+          row_entry(op, tb, i, m, r.idx[m], j, h);
+          term(tr, ti, h, ld(in + (size_t)j * V + v), row_xx(op, tb, i, m, r.idx[m]));
+        }
+      }
+      finish(g, tr, ti);
+    });
+  } else {
+    for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+         g += (size_t)gridDim.x * kBlock) {
+      const int i = (int)(g / V);
+      const int v = (int)(g % V);
+      const int cnt = op.uniform ? op.z : op.nn[i];
+      double tr = 0.0, ti = 0.0;
+      for (int m = 0; m < cnt; ++m) {
+        const size_t e = (size_t)m * op.n + i;
+        int j, c;
+        double2 h;
+        ell_entry(op, tb, e, i, j, h, c);
+        term(tr, ti, h, ld(in + (size_t)j * V + v), ell_xx(op, tb, e, c));
+      }
+      finish(g, tr, ti);
     }
   }
 }
@@ -803,15 +1109,15 @@ __global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
                                                   OT2* __restrict__ out, double bessel,
                                                   int label)
 {
+  const Tables tb = load_tables(op);
   const size_t total = (size_t)op.n * V;
-  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
-       g += (size_t)gridDim.x * kBlock) {
+  auto item = [&](size_t g, auto&& row) {
     const int i = (int)(g / V);
     const int v = (int)(g % V);
     const double p = op.pot[i];
     const double2 x = ld(s1 + g);
     double tr = A::mul(p, x.x), ti = A::mul(p, x.y);
-    hop_row<V, Z, A>(op, i, v, s1, tr, ti);
+    row(i, v, tr, ti);
     tr = A::scale(tr, op);
     ti = A::scale(ti, op);
     const double2 y0 = ld(s0 + g);
@@ -819,6 +1125,19 @@ __global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
     ti = A::two_x_minus(ti, y0.y);
     st(out + g, accumulate<A>(ld(out + g), bessel, tr, ti, label));
     st(s2 + g, make_double2(tr, ti));
+  };
+  if constexpr (Z > 0) {
+    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+      item(g, [&](int i, int v, double& tr, double& ti) {
+        hop_row_pre<V, Z, A>(op, tb, i, v, r, s1, tr, ti);
+      });
+    });
+  } else {
+    for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+         g += (size_t)gridDim.x * kBlock)
+      item(g, [&](int i, int v, double& tr, double& ti) {
+        hop_row<V, Z, A>(op, tb, i, v, s1, tr, ti);
+      });
   }
 }
 
@@ -832,41 +1151,27 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
                                                    VT2* s2x, OT2* __restrict__ out,
                                                    double bessel, int label)
 {
+  const Tables tb = load_tables(op);
   const size_t total = (size_t)op.n * V;
-  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
-       g += (size_t)gridDim.x * kBlock) {
+  auto item = [&](size_t g, auto&& row) {
     const int i = (int)(g / V);
     const int v = (int)(g % V);
     const double p = op.pot[i];
     const double2 a1 = ld(s1 + g), a1x = ld(s1x + g);
     double tr = A::mul(p, a1.x), ti = A::mul(p, a1.y);
     double txr = A::mul(p, a1x.x), txi = A::mul(p, a1x.y);
-    const int cnt = op.uniform ? op.z : op.nn[i];
-    auto body = [&](int m) {
-      const size_t e = (size_t)m * op.n + i;
-      const int j = op.nl[e];
-      const double2 h = op.hop[e];
-      const double2 c = ld(s1 + (size_t)j * V + v);
-      const double2 cx = ld(s1x + (size_t)j * V + v);
+    // One neighbour term of both recurrences, in the reference's order.
+    auto term = [&](double2 h, double2 c, double2 cx, double x) {
       const double hre = A::cre(h.x, h.y, c.x, c.y);
       const double him = A::cim(h.x, h.y, c.x, c.y);
       tr = A::add(tr, hre);
       ti = A::add(ti, him);
       txr = A::add(txr, A::cre(h.x, h.y, cx.x, cx.y));
       txi = A::add(txi, A::cim(h.x, h.y, cx.x, cx.y));
-      const double x = op.xx[e];
       txr = A::sub(txr, A::mul(hre, x));
       txi = A::sub(txi, A::mul(him, x));
     };
-    if constexpr (Z > 0) {
-#pragma unroll
-      for (int m = 0; m < Z; ++m)
-        if (m < cnt)
-          body(m);
-    } else {
-      for (int m = 0; m < cnt; ++m)
-        body(m);
-    }
+    row(i, v, term);
     const double2 y0 = ld(s0 + g), y0x = ld(s0x + g);
     tr = A::two_x_minus(A::scale(tr, op), y0.x);
     ti = A::two_x_minus(A::scale(ti, op), y0.y);
@@ -875,6 +1180,35 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
     st(s2 + g, make_double2(tr, ti));
     st(s2x + g, make_double2(txr, txi));
     st(out + g, accumulate<A>(ld(out + g), bessel, txr, txi, label));
+  };
+  if constexpr (Z > 0) {
+    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+      item(g, [&](int i, int v, auto&& term) {
+#pragma unroll
+        for (int m = 0; m < Z; ++m) {
+          if (m < r.cnt) {
+            int j;
+            double2 h;
+            row_entry(op, tb, i, m, r.idx[m], j, h);
+            term(h, ld(s1 + (size_t)j * V + v), ld(s1x + (size_t)j * V + v),
+                 row_xx(op, tb, i, m, r.idx[m]));
+          }
+        }
+      });
+    });
+  } else {
+    for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+         g += (size_t)gridDim.x * kBlock)
+      item(g, [&](int i, int v, auto&& term) {
+        const int cnt = op.uniform ? op.z : op.nn[i];
+        for (int m = 0; m < cnt; ++m) {
+          const size_t e = (size_t)m * op.n + i;
+          int j, c;
+          double2 h;
+          ell_entry(op, tb, e, i, j, h, c);
+          term(h, ld(s1 + (size_t)j * V + v), ld(s1x + (size_t)j * V + v), ell_xx(op, tb, e, c));
+        }
+      });
   }
 }
 

@@ -185,7 +185,7 @@ extern "C" gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, con
   if (e != cudaSuccess)
     return gqt::cuda_fail(e, "cudaMemsetAsync(counter)", __FILE__, __LINE__);
 
-  Op op;
+  Op op{};  // the ELL arrays (no coded table: this launch has no dynamic shared memory)
   op.n = h->n;
   op.z = h->z;
   op.uniform = h->uniform;
@@ -196,6 +196,7 @@ extern "C" gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, con
   op.xx = h->xx;
   op.emax = h->energy_max;
   op.inv_emax = 1.0 / h->energy_max;
+  op.lib_div = !(h->energy_max >= 0x1p-100 && h->energy_max <= 0x1p100);
   const double2* a0 = mode == 1 ? (const double2*)t0->data : nullptr;
   const double2* a1 = (const double2*)t1->data;
   double2* o = (double2*)out->data;

@@ -325,6 +325,10 @@ gqt_ham::~gqt_ham()
   cudaFree(xx);
   cudaFree(pot);
   cudaFree(tile_first);
+  cudaFree(code);
+  cudaFree(code_delta);
+  cudaFree(code_hop);
+  cudaFree(code_xx);
 }
 
 namespace {
@@ -413,6 +417,53 @@ void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
   }
 }
 
+// The dictionary of (j - i, hopping, xx) over every ELL entry, padding entries
+// included; false when it would exceed GQT_MAX_CODES entries.
+bool build_codes(const Packed& P, std::vector<uint8_t>& codes, std::vector<int>& delta,
+                 std::vector<double2>& hop, std::vector<double>& xx)
+{
+  struct Key {
+    long long d;
+    uint64_t hr, hi, x;
+    bool operator==(const Key& o) const
+    {
+      return d == o.d && hr == o.hr && hi == o.hi && x == o.x;
+    }
+  };
+  struct KeyHash {
+    size_t operator()(const Key& k) const
+    {
+      uint64_t h = (uint64_t)k.d * 0x9e3779b97f4a7c15ull;
+      h ^= k.hr + 0x7f4a7c159e3779b9ull + (h << 6) + (h >> 2);
+      h ^= k.hi + 0x94d049bb133111ebull + (h << 6) + (h >> 2);
+      h ^= k.x + 0xbf58476d1ce4e5b9ull + (h << 6) + (h >> 2);
+      return (size_t)h;
+    }
+  };
+  std::unordered_map<Key, int, KeyHash> dict;
+  codes.assign((size_t)P.n * P.z, 0);
+  for (int m = 0; m < P.z; ++m)
+    for (int i = 0; i < P.n; ++i) {
+      const size_t e = (size_t)m * P.n + i;
+      Key k;
+      k.d = (long long)P.nl[e] - i;
+      std::memcpy(&k.hr, &P.hop[e].x, 8);
+      std::memcpy(&k.hi, &P.hop[e].y, 8);
+      std::memcpy(&k.x, &P.xx[e], 8);
+      auto it = dict.find(k);
+      if (it == dict.end()) {
+        if ((int)dict.size() == GQT_MAX_CODES)
+          return false;
+        it = dict.emplace(k, (int)dict.size()).first;
+        delta.push_back((int)k.d);
+        hop.push_back(P.hop[e]);
+        xx.push_back(P.xx[e]);
+      }
+      codes[e] = (uint8_t)it->second;
+    }
+  return true;
+}
+
 gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
 {
   const size_t pairs = (size_t)P.n * P.z;
@@ -435,6 +486,23 @@ gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ha
   GQT_CUDA(cudaMemcpy(h->xx, P.xx.data(), pairs * sizeof(double), cudaMemcpyHostToDevice));
   GQT_CUDA(cudaMemcpy(h->pot, P.pot.data(), (size_t)P.n * sizeof(double),
                       cudaMemcpyHostToDevice));
+  std::vector<uint8_t> codes;
+  std::vector<int> delta;
+  std::vector<double2> chop;
+  std::vector<double> cxx;
+  if (build_codes(P, codes, delta, chop, cxx)) {
+    const size_t nc = delta.size();
+    GQT_CUDA(cudaMalloc(&h->code, pairs));
+    GQT_CUDA(cudaMalloc(&h->code_delta, nc * sizeof(int)));
+    GQT_CUDA(cudaMalloc(&h->code_hop, nc * sizeof(double2)));
+    GQT_CUDA(cudaMalloc(&h->code_xx, nc * sizeof(double)));
+    GQT_CUDA(cudaMemcpy(h->code, codes.data(), pairs, cudaMemcpyHostToDevice));
+    GQT_CUDA(cudaMemcpy(h->code_delta, delta.data(), nc * sizeof(int), cudaMemcpyHostToDevice));
+    GQT_CUDA(cudaMemcpy(h->code_hop, chop.data(), nc * sizeof(double2), cudaMemcpyHostToDevice));
+    GQT_CUDA(cudaMemcpy(h->code_xx, cxx.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
+    h->n_codes = (int)nc;
+    h->use_codes = 1;
+  }
   h->ws.reset(new_workspace());
   return GQT_OK;
 }
@@ -514,6 +582,39 @@ extern "C" gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count,
   GQT_CUDA(cudaMemcpy(h->tile_first, first.data(), first.size() * sizeof(int),
                       cudaMemcpyHostToDevice));
   *out = guard.release();
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_set_format(gqt_ham* h, int format)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_format: null handle");
+  if (format != GQT_FORMAT_ELL && format != GQT_FORMAT_CODED)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_format: unknown format %d", format);
+  if (format == GQT_FORMAT_CODED && !h->code)
+    return fail(GQT_ERR_STATE,
+                "gqt_ham_set_format: the operator has more than %d distinct entries",
+                GQT_MAX_CODES);
+  const int want = format == GQT_FORMAT_CODED ? 1 : 0;
+  if (want != h->use_codes && h->ws) {
+    // Graphs captured so far launch the other format's reads.
+    cudaStreamSynchronize(t_stream);
+    for (auto& kv : h->ws->graphs)
+      cudaGraphExecDestroy(kv.second);
+    h->ws->graphs.clear();
+  }
+  h->use_codes = want;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_format(const gqt_ham* h, int* format, int* n_codes)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_format: null handle");
+  if (format)
+    *format = h->use_codes ? GQT_FORMAT_CODED : GQT_FORMAT_ELL;
+  if (n_codes)
+    *n_codes = h->n_codes;
   return GQT_OK;
 }
 

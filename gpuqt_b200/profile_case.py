@@ -4,7 +4,9 @@
 
 Builds the workload's lattice, then runs `sets` moment sets of `moments` moments in
 one arithmetic form: fp64 (plain, one vector), fp32v1, or fp32vV (V vectors per
-launch, FP32 storage). Prints one JSON line with the measured rate.
+launch, FP32 storage), with the operator in the coded format (the default where the
+lattice has one) or in the plain ELL arrays (`--format ell`). Prints one JSON line
+with the measured rate.
 """
 from __future__ import annotations
 
@@ -26,6 +28,7 @@ def main() -> None:
     ap.add_argument("--form", default="fp64")
     ap.add_argument("--moments", type=int, default=20)
     ap.add_argument("--sets", type=int, default=2)
+    ap.add_argument("--format", default="default", choices=["default", "ell", "coded"])
     ap.add_argument("--autotune", action="store_true",
                     help="let the autotuner pick the shape for this vector count first")
     args = ap.parse_args()
@@ -58,6 +61,8 @@ def main() -> None:
             X = g.Vector.from_host(np.stack([v[0] for v in vecs]),
                                    np.stack([v[1] for v in vecs]), nvec=V, precision=prec)
             sites = m.n
+        if args.format != "default":
+            H.set_format(g.FORMAT_ELL if args.format == "ell" else g.FORMAT_CODED)
         tuned = None
         if args.autotune:
             tuned = g.autotune_nvec(H, prec, 20, [V])[1]
@@ -75,6 +80,8 @@ def main() -> None:
         torch.cuda.synchronize()
         s = a.elapsed_time(b) / 1e3
         print(json.dumps({"workload": args.workload, "form": args.form, "sites": sites,
+                          "format": "coded" if H.format == g.FORMAT_CODED else "ell",
+                          "n_codes": H.n_codes,
                           "moments": args.moments, "sets": args.sets, "autotune": tuned,
                           "site_moments_per_s": V * sites * args.moments * args.sets / s}))
     finally:

@@ -85,6 +85,20 @@ gqt_status gqt_ham_destroy(gqt_ham* h);
 gqt_status gqt_ham_info(const gqt_ham* h, int* n, int* max_neighbor, int* uniform_rows,
                         double* energy_max);
 
+/* Operator storage formats (no counterpart in the reference, whose device layout is
+ * GQT_FORMAT_ELL). When the entries (j - i, hopping, xx) of the ELL take at most
+ * GQT_MAX_CODES distinct values — lattice models do — gqt_ham_create also builds the
+ * coded form: one byte per entry into a table of those values, which the kernels
+ * read from shared memory. The arithmetic is unchanged (the same doubles in the same
+ * order, so the FP64 form stays bit-identical to the reference); the operator's bytes
+ * per site drop from 20 z to z. The coded form is used by default when it exists;
+ * gqt_ham_set_format selects a format, gqt_ham_format reports the one in use and the
+ * table size (0 when there is no coded form). */
+#define GQT_MAX_CODES 256
+enum { GQT_FORMAT_ELL = 0, GQT_FORMAT_CODED = 1 };
+gqt_status gqt_ham_set_format(gqt_ham* h, int format);
+gqt_status gqt_ham_format(const gqt_ham* h, int* format, int* n_codes);
+
 /* Realisation batches (no counterpart in the reference, which runs one model per
  * process): `count` independent models — disorder realisations, lattices of uneven
  * sizes — as one block-diagonal operator, so one launch per Chebyshev step advances

@@ -162,3 +162,29 @@ def test_errors_do_not_crash():
     with pytest.raises(g.GqtError):
         g.chebyshev_1x(H, y32, y32, 1.0)     # single terms take FP64 vectors
     g.sync()
+
+
+@pytest.mark.parametrize("emax", [8.7, 5.0, 3.0000000000000004, 13.2, 1.0, 0.1, 7.3e5, 2.0 ** -120])
+def test_division_by_energy_max_correctly_rounded(emax):
+    """The FP64 form's a / E_max (FMA-based, library division at the range edges)
+    against IEEE division on the host: a site with no neighbours and potential a,
+    applied to x = 1, gives a / E_max. Random significands over the whole exponent
+    range, subnormals, zeros of both signs and infinities."""
+    rng = np.random.default_rng(int(emax * 1000) % 2**31)
+    n = 1 << 20
+    a = rng.uniform(1.0, 2.0, n) * np.exp2(rng.integers(-1074, 1024, n).astype(np.float64))
+    a[: n // 2] = rng.uniform(-16.0, 16.0, n // 2)  # the operator's own range
+    a *= np.where(rng.random(n) < 0.5, -1.0, 1.0)
+    a[:8] = [0.0, -0.0, np.inf, -np.inf, 5e-324, -2.2250738585072014e-308, 1.7e308, 1.0]
+    H = g.Hamiltonian(n=n, max_neighbor=1, energy_max=emax,
+                      neighbor_number=np.zeros(n, np.int32),
+                      neighbor_list=np.arange(n, dtype=np.int32), potential=a,
+                      hopping_real=np.zeros(n), hopping_imag=np.zeros(n))
+    x = g.Vector.from_host(np.ones(n), np.zeros(n))
+    y = g.Vector(n)
+    g.apply(H, x, y)
+    re, _ = y.download()
+    with np.errstate(over="ignore", under="ignore"):
+        want = a / emax
+    np.testing.assert_array_equal(re, want)
+    assert np.array_equal(np.signbit(re), np.signbit(want))
