@@ -10,14 +10,11 @@
 
 namespace gqt {
 
-struct FormOps {
-  int precision;
-  int nvec;
-  size_t elem_bytes;  // bytes of one complex vector element
+// The kernels that read the operator, for one format (ELL arrays or coded table).
+struct OpFns {
   // out = H t1 (mode kApply) or 2 H t1 - t0 (kCheb); dot != nullptr fuses <left|out>.
   gqt_status (*step)(const Op& op, int mode, const void* t0, const void* t1, void* out,
                      const void* left, const Dot* dot);
-  gqt_status (*dot)(size_t total, const void* state, const void* left, const Dot& dot);
   // One step of a realisation batch (mode kDotOnly, kApply or kCheb) with moments per
   // realisation.
   gqt_status (*step_multi)(const Op& op, int mode, const void* t0, const void* t1, void* out,
@@ -25,22 +22,61 @@ struct FormOps {
   gqt_status (*xop)(const Op& op, bool current, const void* in, void* out);
   // Evolution terms; out is a double2 accumulator (the FP64 state itself, or the
   // FP32 form's FP64 accumulator).
-  gqt_status (*cheb01)(size_t total, const void* s0, const void* s1, double2* out, double b0,
-                       double b1);
   gqt_status (*cheb2)(const Op& op, const void* s0, const void* s1, void* s2, double2* out,
                       double bessel, int label);
-  gqt_status (*cheb1x)(size_t total, const void* s1x, double2* out, double b1);
   gqt_status (*cheb2x)(const Op& op, const void* s0, const void* s0x, const void* s1,
                        const void* s1x, void* s2, void* s2x, double2* out, double bessel,
                        int label);
+};
+
+struct FormOps {
+  int precision;
+  int nvec;
+  size_t elem_bytes;  // bytes of one complex vector element
+  OpFns fmt[2];       // [0]: ELL arrays, [1]: coded table
+  gqt_status (*dot)(size_t total, const void* state, const void* left, const Dot& dot);
+  gqt_status (*cheb01)(size_t total, const void* s0, const void* s1, double2* out, double b0,
+                       double b1);
+  gqt_status (*cheb1x)(size_t total, const void* s1x, double2* out, double b1);
   gqt_status (*add)(size_t total, void* dst, const void* src);
   gqt_status (*apply_sz)(size_t total, int nvec, void* dst, const void* src);
   gqt_status (*interleave)(int n, int nvec, const double* re, const double* im, void* out);
   gqt_status (*deinterleave)(int n, int nvec, const void* in, double* re, double* im);
+
+  // The operator kernels of op's format.
+  const OpFns& of(const Op& op) const { return fmt[op.code != nullptr ? 1 : 0]; }
+  gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                  const void* left, const Dot* d) const
+  {
+    return of(op).step(op, mode, t0, t1, out, left, d);
+  }
+  gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                        const void* left, const MultiDot& md) const
+  {
+    return of(op).step_multi(op, mode, t0, t1, out, left, md);
+  }
+  gqt_status xop(const Op& op, bool current, const void* in, void* out) const
+  {
+    return of(op).xop(op, current, in, out);
+  }
+  gqt_status cheb2(const Op& op, const void* s0, const void* s1, void* s2, double2* out,
+                   double bessel, int label) const
+  {
+    return of(op).cheb2(op, s0, s1, s2, out, bessel, label);
+  }
+  gqt_status cheb2x(const Op& op, const void* s0, const void* s0x, const void* s1,
+                    const void* s1x, void* s2, void* s2x, double2* out, double bessel,
+                    int label) const
+  {
+    return of(op).cheb2x(op, s0, s0x, s1, s1x, s2, s2x, out, bessel, label);
+  }
 };
 
 const FormOps* forms_fp64(int nvec);
 const FormOps* forms_fp32(int nvec);
+// The coded format's operator kernels (gqt_forms_fp64_coded.cu, gqt_forms_fp32_coded.cu).
+OpFns op_fns_fp64_coded(int nvec);
+OpFns op_fns_fp32_coded(int nvec);
 inline const FormOps* form_ops(int precision, int nvec)
 {
   if (precision == GQT_FP64)

@@ -7,15 +7,15 @@ const FormOps* forms_fp32(int nvec)
 {
   switch (nvec) {
     case 1:
-      return FormImpl<float2, 1, FastArith>::table(GQT_FP32);
+      return FormImpl<float2, 1, FastArith>::table(GQT_FP32, op_fns_fp32_coded(1));
     case 4:
-      return FormImpl<float2, 4, FastArith>::table(GQT_FP32);
+      return FormImpl<float2, 4, FastArith>::table(GQT_FP32, op_fns_fp32_coded(4));
     case 8:
-      return FormImpl<float2, 8, FastArith>::table(GQT_FP32);
+      return FormImpl<float2, 8, FastArith>::table(GQT_FP32, op_fns_fp32_coded(8));
     case 16:
-      return FormImpl<float2, 16, FastArith>::table(GQT_FP32);
+      return FormImpl<float2, 16, FastArith>::table(GQT_FP32, op_fns_fp32_coded(16));
     case 32:
-      return FormImpl<float2, 32, FastArith>::table(GQT_FP32);
+      return FormImpl<float2, 32, FastArith>::table(GQT_FP32, op_fns_fp32_coded(32));
     default:
       return nullptr;
   }

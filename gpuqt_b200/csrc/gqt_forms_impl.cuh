@@ -1,5 +1,7 @@
-// Template bodies of the launch tables; included by gqt_forms_fp64.cu and
-// gqt_forms_fp32.cu only.
+// Template bodies of the launch tables; included by the gqt_forms_*.cu files only.
+// OpImpl holds the kernels that read the operator, instantiated once per format
+// (C: coded table, or the ELL arrays) in their own translation units; FormImpl holds
+// the rest and assembles the table.
 #pragma once
 
 #include <type_traits>
@@ -63,8 +65,8 @@ constexpr int vectors_per_thread()
   return V < w ? V : w;
 }
 
-template <typename VT2, int V, class A>
-struct FormImpl {
+template <typename VT2, int V, class A, bool C>
+struct OpImpl {
   // Default vectors per thread, and the alternative the autotuner may choose (two
   // vectors per thread: half the accumulator registers, twice the threads per site).
   static constexpr int W = vectors_per_thread<VT2, V>();
@@ -88,14 +90,14 @@ struct FormImpl {
           const size_t items = (size_t)op.n * (V / WW);
           if (mode == kApply) {
             if (dot)
-              return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, true>, items, op, a0, a1, o, l,
+              return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, true, C>, items, op, a0, a1, o, l,
                             d);
-            return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, false>, items, op, a0, a1, o, l,
+            return launch_op(k_step_vec<VT2, V, WW, Z, A, kApply, false, C>, items, op, a0, a1, o, l,
                           d);
           }
           if (dot)
-            return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, true>, items, op, a0, a1, o, l, d);
-          return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, false>, items, op, a0, a1, o, l, d);
+            return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, true, C>, items, op, a0, a1, o, l, d);
+          return launch_op(k_step_vec<VT2, V, WW, Z, A, kCheb, false, C>, items, op, a0, a1, o, l, d);
         };
         if constexpr (W2 != W) {
           if (op.wpt == W2)
@@ -105,12 +107,12 @@ struct FormImpl {
       }
       if (mode == kApply) {
         if (dot)
-          return launch_op(k_step<VT2, V, Z, A, kApply, true>, total, op, a0, a1, o, l, d);
-        return launch_op(k_step<VT2, V, Z, A, kApply, false>, total, op, a0, a1, o, l, d);
+          return launch_op(k_step<VT2, V, Z, A, kApply, true, C>, total, op, a0, a1, o, l, d);
+        return launch_op(k_step<VT2, V, Z, A, kApply, false, C>, total, op, a0, a1, o, l, d);
       }
       if (dot)
-        return launch_op(k_step<VT2, V, Z, A, kCheb, true>, total, op, a0, a1, o, l, d);
-      return launch_op(k_step<VT2, V, Z, A, kCheb, false>, total, op, a0, a1, o, l, d);
+        return launch_op(k_step<VT2, V, Z, A, kCheb, true, C>, total, op, a0, a1, o, l, d);
+      return launch_op(k_step<VT2, V, Z, A, kCheb, false, C>, total, op, a0, a1, o, l, d);
     });
   }
 
@@ -135,10 +137,10 @@ struct FormImpl {
       auto pick = [&](auto wc) -> gqt_status {
         constexpr int WW = decltype(wc)::value;
         if (mode == kDotOnly)
-          return go(k_step_multi<VT2, V, WW, Z, A, kDotOnly>);
+          return go(k_step_multi<VT2, V, WW, Z, A, kDotOnly, C>);
         if (mode == kApply)
-          return go(k_step_multi<VT2, V, WW, Z, A, kApply>);
-        return go(k_step_multi<VT2, V, WW, Z, A, kCheb>);
+          return go(k_step_multi<VT2, V, WW, Z, A, kApply, C>);
+        return go(k_step_multi<VT2, V, WW, Z, A, kCheb, C>);
       };
       if constexpr (W2 != W) {
         if (op.wpt == W2)
@@ -152,27 +154,15 @@ struct FormImpl {
     return GQT_OK;
   }
 
-  static gqt_status dot(size_t total, const void* state, const void* left, const Dot& d)
-  {
-    return launch(k_dot<VT2, V>, total, total, (const VT2*)state, (const VT2*)left, d);
-  }
-
   static gqt_status xop(const Op& op, bool current, const void* in, void* out)
   {
     const size_t total = (size_t)op.n * V;
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
       if (current)
-        return launch_op(k_xop<VT2, V, Z, A, true>, total, op, (const VT2*)in, (VT2*)out);
-      return launch_op(k_xop<VT2, V, Z, A, false>, total, op, (const VT2*)in, (VT2*)out);
+        return launch_op(k_xop<VT2, V, Z, A, true, C>, total, op, (const VT2*)in, (VT2*)out);
+      return launch_op(k_xop<VT2, V, Z, A, false, C>, total, op, (const VT2*)in, (VT2*)out);
     });
-  }
-
-  static gqt_status cheb01(size_t total, const void* s0, const void* s1, double2* out,
-                           double b0, double b1)
-  {
-    return launch(k_cheb01<VT2, double2, A>, total, total, (const VT2*)s0, (const VT2*)s1,
-                  out, b0, b1);
   }
 
   static gqt_status cheb2(const Op& op, const void* s0, const void* s1, void* s2,
@@ -181,14 +171,9 @@ struct FormImpl {
     const size_t total = (size_t)op.n * V;
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
-      return launch_op(k_cheb2<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+      return launch_op(k_cheb2<VT2, double2, V, Z, A, C>, total, op, (const VT2*)s0,
                     (const VT2*)s1, (VT2*)s2, out, bessel, label);
     });
-  }
-
-  static gqt_status cheb1x(size_t total, const void* s1x, double2* out, double b1)
-  {
-    return launch(k_cheb1x<VT2, double2, A>, total, total, (const VT2*)s1x, out, b1);
   }
 
   static gqt_status cheb2x(const Op& op, const void* s0, const void* s0x, const void* s1,
@@ -198,10 +183,32 @@ struct FormImpl {
     const size_t total = (size_t)op.n * V;
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
-      return launch_op(k_cheb2x<VT2, double2, V, Z, A>, total, op, (const VT2*)s0,
+      return launch_op(k_cheb2x<VT2, double2, V, Z, A, C>, total, op, (const VT2*)s0,
                     (const VT2*)s0x, (const VT2*)s1, (const VT2*)s1x, (VT2*)s2, (VT2*)s2x,
                     out, bessel, label);
     });
+  }
+
+  static OpFns fns() { return OpFns{step, step_multi, xop, cheb2, cheb2x}; }
+};
+
+template <typename VT2, int V, class A>
+struct FormImpl {
+  static gqt_status dot(size_t total, const void* state, const void* left, const Dot& d)
+  {
+    return launch(k_dot<VT2, V>, total, total, (const VT2*)state, (const VT2*)left, d);
+  }
+
+  static gqt_status cheb01(size_t total, const void* s0, const void* s1, double2* out,
+                           double b0, double b1)
+  {
+    return launch(k_cheb01<VT2, double2, A>, total, total, (const VT2*)s0, (const VT2*)s1,
+                  out, b0, b1);
+  }
+
+  static gqt_status cheb1x(size_t total, const void* s1x, double2* out, double b1)
+  {
+    return launch(k_cheb1x<VT2, double2, A>, total, total, (const VT2*)s1x, out, b1);
   }
 
   static gqt_status add(size_t total, void* dst, const void* src)
@@ -224,11 +231,26 @@ struct FormImpl {
     return launch(k_deinterleave<VT2>, (size_t)n * nvec, n, nvec, (const VT2*)in, re, im);
   }
 
-  static const FormOps* table(int precision)
+  // The table of this form: the ELL kernels from OpImpl<..., false> (this
+  // translation unit) and the coded ones from their own unit.
+  static const FormOps* table(int precision, OpFns coded)
   {
-    static const FormOps t = {precision, V,      sizeof(VT2), step,  dot, step_multi, xop,
-                              cheb01,    cheb2,  cheb1x,      cheb2x,   add,      apply_sz,
-                              interleave, deinterleave};
+    static const FormOps t = [&] {
+      FormOps f{};
+      f.precision = precision;
+      f.nvec = V;
+      f.elem_bytes = sizeof(VT2);
+      f.fmt[0] = OpImpl<VT2, V, A, false>::fns();
+      f.fmt[1] = coded;
+      f.dot = dot;
+      f.cheb01 = cheb01;
+      f.cheb1x = cheb1x;
+      f.add = add;
+      f.apply_sz = apply_sz;
+      f.interleave = interleave;
+      f.deinterleave = deinterleave;
+      return f;
+    }();
     return &t;
   }
 };

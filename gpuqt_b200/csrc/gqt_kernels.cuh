@@ -60,8 +60,9 @@ struct Dot {
 
 // ------------------------------------------------------------------ operator entries
 // The coded operator's table, staged in dynamic shared memory at kernel start
-// (n_codes * 28 bytes, passed at launch as op_smem_bytes). `op.code` is the same for
-// every thread, so the branches below never diverge.
+// (n_codes * 28 bytes, passed at launch as op_smem_bytes). Every kernel that reads the
+// operator is compiled once per format: C = true reads the codes and the table, C =
+// false the ELL arrays.
 struct Tables {
   const int* delta;
   const double2* hop;
@@ -70,10 +71,11 @@ struct Tables {
 
 inline size_t op_smem_bytes(const Op& op) { return op.code ? (size_t)op.n_codes * 28 : 0; }
 
+template <bool C>
 __device__ __forceinline__ Tables load_tables(const Op& op)
 {
   extern __shared__ __align__(16) unsigned char dyn_smem[];
-  if (!op.code)
+  if constexpr (!C)
     return Tables{nullptr, nullptr, nullptr};
   const int n = op.n_codes;
   double2* hop = reinterpret_cast<double2*>(dyn_smem);
@@ -90,10 +92,11 @@ __device__ __forceinline__ Tables load_tables(const Op& op)
 
 // Entry e = m * n + i of row i: neighbour j, hopping h, and the table row c (coded
 // form only) for ell_xx.
+template <bool C>
 __device__ __forceinline__ void ell_entry(const Op& op, const Tables& tb, size_t e, int i,
                                           int& j, double2& h, int& c)
 {
-  if (tb.hop) {
+  if constexpr (C) {
     c = op.code[e];
     j = i + tb.delta[c];
     h = tb.hop[c];
@@ -104,9 +107,13 @@ __device__ __forceinline__ void ell_entry(const Op& op, const Tables& tb, size_t
   }
 }
 
+template <bool C>
 __device__ __forceinline__ double ell_xx(const Op& op, const Tables& tb, size_t e, int c)
 {
-  return tb.hop ? tb.xx[c] : op.xx[e];
+  if constexpr (C)
+    return tb.xx[c];
+  else
+    return op.xx[e];
 }
 
 // ------------------------------------------------------------------ arithmetic
@@ -392,9 +399,24 @@ __device__ __forceinline__ void stw(double2* p, const double2 (&v)[W])
 }
 
 // ------------------------------------------------------------------ the operator row
+// f(m) for the entries m < cnt of a row, unrolled when the bound Z is known.
+template <int Z, class F>
+__device__ __forceinline__ void for_entries(int cnt, F&& f)
+{
+  if constexpr (Z > 0) {
+#pragma unroll
+    for (int m = 0; m < Z; ++m)
+      if (m < cnt)
+        f(m);
+  } else {
+    for (int m = 0; m < cnt; ++m)
+      f(m);
+  }
+}
+
 // acc += sum_m H_im x_{j_m} for one (site i, vector v), neighbours in ELL order.
 // Z > 0: the row length bound is known at compile time and the loop is unrolled.
-template <int V, int Z, class A, typename VT2>
+template <int V, int Z, class A, bool C, typename VT2>
 __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, int v,
                                         const VT2* __restrict__ x, double& tr, double& ti)
 {
@@ -406,7 +428,7 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
         const size_t e = (size_t)m * op.n + i;
         int j, c;
         double2 h;
-        ell_entry(op, tb, e, i, j, h, c);
+        ell_entry<C>(op, tb, e, i, j, h, c);
         const double2 y = ld(x + (size_t)j * V + v);
         tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
         ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
@@ -417,7 +439,7 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
       const size_t e = (size_t)m * op.n + i;
       int j, c;
       double2 h;
-      ell_entry(op, tb, e, i, j, h, c);
+      ell_entry<C>(op, tb, e, i, j, h, c);
       const double2 y = ld(x + (size_t)j * V + v);
       tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
       ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
@@ -427,9 +449,41 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
 
 enum StepMode { kApply = 0, kCheb = 1 };
 
-#ifndef GQT_STEP_PREFETCH
-#define GQT_STEP_PREFETCH 2
+// Grid-stride loop shape of each operator kernel, per format (C), storage type and
+// row bound Z. The pipelined loop loads the next element's row (and, in k_step, its
+// streamed inputs) one iteration ahead, so an iteration waits on one memory round
+// trip instead of two; it costs registers, hence resident warps. Chosen from B200
+// measurements (graphene 2,097,152 sites, square 1,048,576, cubic 16,777,216): the
+// step gains 10-60 % from it in both formats (with its register budget fixed by
+// step_min_blocks); the other coded kernels 10-50 % (the evolution term k_cheb2
+// excepted); the other ELL kernels lose. GQT_PIPELINE = 0 or 1 at compile time
+// forces one loop shape everywhere.
+#ifndef GQT_PIPELINE
+#define GQT_PIPELINE -1
 #endif
+enum PipeKernel { kPipeStep, kPipeStepVec, kPipeStepMulti, kPipeXop, kPipeCheb2, kPipeCheb2x };
+
+template <int K, bool C, typename VT2, int Z>
+__host__ __device__ constexpr bool pipelined()
+{
+  if constexpr (Z <= 0) {
+    return false;  // the pipelined loops need the row bound at compile time
+  } else if constexpr (GQT_PIPELINE >= 0) {
+    return GQT_PIPELINE > 0;
+  } else {
+    switch (K) {
+      case kPipeStep:
+        return true;
+      case kPipeStepVec:
+      case kPipeStepMulti:
+      case kPipeXop:
+      case kPipeCheb2x:
+        return C;
+      default:
+        return false;
+    }
+  }
+}
 
 // One site's row, fetched one grid-stride iteration ahead of its use: the row length
 // and the table rows (coded form) or neighbour indices (ELL form) of its Z entries.
@@ -440,20 +494,23 @@ struct RowIdx {
   int idx[Z];
 };
 
-template <int Z>
-__device__ __forceinline__ void fetch_row(const Op& op, const Tables& tb, int i, RowIdx<Z>& r)
+template <int Z, bool C>
+__device__ __forceinline__ void fetch_row(const Op& op, int i, RowIdx<Z>& r)
 {
   r.cnt = op.uniform ? Z : op.nn[i];
 #pragma unroll
   for (int m = 0; m < Z; ++m) {
     const size_t e = (size_t)m * op.n + i;
-    r.idx[m] = tb.hop ? (int)op.code[e] : op.nl[e];
+    if constexpr (C)
+      r.idx[m] = op.code[e];
+    else
+      r.idx[m] = op.nl[e];
   }
 }
 
 // hop_row from a prefetched row: every gather is issued before the arithmetic, which
 // keeps the reference's neighbour order.
-template <int V, int Z, class A, typename VT2>
+template <int V, int Z, class A, bool C, typename VT2>
 __device__ __forceinline__ void hop_row_pre(const Op& op, const Tables& tb, int i, int v,
                                             const RowIdx<Z>& r, const VT2* __restrict__ x,
                                             double& tr, double& ti)
@@ -462,7 +519,7 @@ __device__ __forceinline__ void hop_row_pre(const Op& op, const Tables& tb, int 
   double2 h[Z], y[Z];
 #pragma unroll
   for (int m = 0; m < Z; ++m) {
-    if (tb.hop) {
+    if constexpr (C) {
       j[m] = i + tb.delta[r.idx[m]];
       h[m] = tb.hop[r.idx[m]];
     } else {
@@ -484,10 +541,11 @@ __device__ __forceinline__ void hop_row_pre(const Op& op, const Tables& tb, int 
 }
 
 // Neighbour j and hopping h of entry m of row i, from its prefetched index.
+template <bool C>
 __device__ __forceinline__ void row_entry(const Op& op, const Tables& tb, int i, int m,
                                           int idx, int& j, double2& h)
 {
-  if (tb.hop) {
+  if constexpr (C) {
     j = i + tb.delta[idx];
     h = tb.hop[idx];
   } else {
@@ -497,7 +555,7 @@ __device__ __forceinline__ void row_entry(const Op& op, const Tables& tb, int i,
 }
 
 // acc[k] += sum_m H_im x_{j_m, v0 + k} for W consecutive vectors, from a prefetched row.
-template <int V, int W, int Z, class A, typename VT2>
+template <int V, int W, int Z, class A, bool C, typename VT2>
 __device__ __forceinline__ void hop_row_w(const Op& op, const Tables& tb, int i, int v0,
                                           const RowIdx<Z>& r, const VT2* __restrict__ x,
                                           double (&tr)[W], double (&ti)[W])
@@ -507,7 +565,7 @@ __device__ __forceinline__ void hop_row_w(const Op& op, const Tables& tb, int i,
     if (m < r.cnt) {
       int j;
       double2 h;
-      row_entry(op, tb, i, m, r.idx[m], j, h);
+      row_entry<C>(op, tb, i, m, r.idx[m], j, h);
       double2 y[W];
       ldw<W>(x + (size_t)j * V + v0, y);
 #pragma unroll
@@ -520,29 +578,71 @@ __device__ __forceinline__ void hop_row_w(const Op& op, const Tables& tb, int i,
 }
 
 // xx of entry m of row i, from its prefetched index.
+template <bool C>
 __device__ __forceinline__ double row_xx(const Op& op, const Tables& tb, int i, int m, int idx)
 {
-  return tb.hop ? tb.xx[idx] : op.xx[(size_t)m * op.n + i];
+  if constexpr (C)
+    return tb.xx[idx];
+  else
+    return op.xx[(size_t)m * op.n + i];
 }
 
 // Runs f(g, row) over this thread's grid-stride items g < total (site g / PER), with
 // each item's row loaded one iteration ahead: an iteration then waits on one memory
 // round trip (its gathers) instead of two (row, then gathers).
-template <int Z, int PER, class F>
-__device__ __forceinline__ void pipelined_rows(const Op& op, const Tables& tb, size_t total,
-                                               F&& f)
+template <int Z, int PER, bool C, class F>
+__device__ __forceinline__ void pipelined_rows(const Op& op, size_t total, F&& f)
 {
   const size_t stride = (size_t)gridDim.x * kBlock;
   size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
   RowIdx<Z> cur;
   if (g < total)
-    fetch_row<Z>(op, tb, (int)(g / PER), cur);
+    fetch_row<Z, C>(op, (int)(g / PER), cur);
   for (; g < total; g += stride) {
     RowIdx<Z> nxt = cur;
     if (g + stride < total)
-      fetch_row<Z>(op, tb, (int)((g + stride) / PER), nxt);
+      fetch_row<Z, C>(op, (int)((g + stride) / PER), nxt);
     f(g, cur);
     cur = nxt;
+  }
+}
+
+// The ELL form's hoppings of one row, loaded one iteration ahead with its indices (the
+// coded form keeps its hoppings in shared memory).
+template <int Z>
+struct RowHop {
+  double2 h[Z];
+};
+template <>
+struct RowHop<0> {};  // coded form: nothing travels
+
+template <int Z>
+__device__ __forceinline__ void fetch_hops(const Op& op, int i, RowHop<Z>& r)
+{
+  if constexpr (Z > 0) {
+#pragma unroll
+    for (int m = 0; m < Z; ++m)
+      r.h[m] = op.hop[(size_t)m * op.n + i];
+  }
+}
+
+// hop_row from a prefetched ELL row and its prefetched hoppings.
+template <int V, int Z, class A, typename VT2>
+__device__ __forceinline__ void hop_row_ahead(int v, const RowIdx<Z>& r, const RowHop<Z>& hr,
+                                              const VT2* __restrict__ x, double& tr,
+                                              double& ti)
+{
+  double2 y[Z];
+#pragma unroll
+  for (int m = 0; m < Z; ++m)
+    if (m < r.cnt)
+      y[m] = ld(x + (size_t)r.idx[m] * V + v);
+#pragma unroll
+  for (int m = 0; m < Z; ++m) {
+    if (m < r.cnt) {
+      tr = A::add(tr, A::cre(hr.h[m].x, hr.h[m].y, y[m].x, y[m].y));
+      ti = A::add(ti, A::cim(hr.h[m].x, hr.h[m].y, y[m].x, y[m].y));
+    }
   }
 }
 
@@ -576,42 +676,56 @@ __device__ __forceinline__ void fetch_streams(const Op& op, size_t g, const VT2*
 // the next element's row indices are loaded while this element's gathers are in
 // flight, so an iteration waits on one memory round trip (the gathers) instead of
 // two (row, then gathers).
-template <typename VT2, int V, int Z, class A, int MODE, bool DOT>
-__global__ void __launch_bounds__(kBlock) k_step(Op op, const VT2* t0,
+// Resident blocks per SM the step is compiled for (its register budget): 3 for rows of
+// up to four entries, 2 for six (the pipelined row of six holds twice the indices).
+// Measured on B200 against the compiler's own choice, which varied from 43 to 114
+// registers between near-identical builds of the same loop.
+template <int Z>
+constexpr int step_min_blocks()
+{
+  return Z >= 6 ? 2 : 3;
+}
+
+template <typename VT2, int V, int Z, class A, int MODE, bool DOT, bool C>
+__global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, const VT2* t0,
                                                  const VT2* __restrict__ t1, VT2* out,
                                                  const VT2* __restrict__ left, Dot dot)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   const size_t total = (size_t)op.n * V;
   const size_t stride = (size_t)gridDim.x * kBlock;
   CSum re{0.0, 0.0}, im{0.0, 0.0};
   size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
-  if constexpr (Z > 0 && GQT_STEP_PREFETCH > 0) {
+  if constexpr (Z > 0 && pipelined<kPipeStep, C, VT2, Z>()) {
     RowIdx<Z> cur;
+    constexpr bool kHops = !C;
+    RowHop<(kHops ? Z : 0)> hc;  // ELL form: the row's hoppings travel with its indices
     Streams sc;
     if (g < total) {
-      fetch_row<Z>(op, tb, (int)(g / V), cur);
-      if constexpr (GQT_STEP_PREFETCH > 1)
-        fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, sc);
+      fetch_row<Z, C>(op, (int)(g / V), cur);
+      if constexpr (kHops)
+        fetch_hops<Z>(op, (int)(g / V), hc);
+      fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, sc);
     }
     for (; g < total; g += stride) {
       const int i = (int)(g / V);
       const int v = (int)(g % V);
       const size_t gn = g + stride;
-      Streams s;
-      if constexpr (GQT_STEP_PREFETCH > 1)
-        s = sc;
-      else
-        fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, s);
+      const Streams s = sc;
       RowIdx<Z> nxt = cur;
+      RowHop<(kHops ? Z : 0)> hn = hc;
       if (gn < total) {
-        fetch_row<Z>(op, tb, (int)(gn / V), nxt);
-        if constexpr (GQT_STEP_PREFETCH > 1)
-          fetch_streams<VT2, V, MODE, DOT>(op, gn, t0, t1, left, sc);
+        fetch_row<Z, C>(op, (int)(gn / V), nxt);
+        if constexpr (kHops)
+          fetch_hops<Z>(op, (int)(gn / V), hn);
+        fetch_streams<VT2, V, MODE, DOT>(op, gn, t0, t1, left, sc);
       }
       double tr = A::mul(s.p, s.x.x);
       double ti = A::mul(s.p, s.x.y);
-      hop_row_pre<V, Z, A>(op, tb, i, v, cur, t1, tr, ti);
+      if constexpr (kHops)
+        hop_row_ahead<V, Z, A>(v, cur, hc, t1, tr, ti);
+      else
+        hop_row_pre<V, Z, A, C>(op, tb, i, v, cur, t1, tr, ti);
       tr = A::scale(tr, op);
       ti = A::scale(ti, op);
       if constexpr (MODE == kCheb) {
@@ -623,6 +737,7 @@ __global__ void __launch_bounds__(kBlock) k_step(Op op, const VT2* t0,
       if constexpr (DOT)
         dot_term(re, im, stored(out, r), s.l);
       cur = nxt;
+      hc = hn;
     }
   } else {
     for (; g < total; g += stride) {
@@ -632,7 +747,7 @@ __global__ void __launch_bounds__(kBlock) k_step(Op op, const VT2* t0,
       const double2 x = ld(t1 + g);
       double tr = A::mul(p, x.x);
       double ti = A::mul(p, x.y);
-      hop_row<V, Z, A>(op, tb, i, v, t1, tr, ti);
+      hop_row<V, Z, A, C>(op, tb, i, v, t1, tr, ti);
       tr = A::scale(tr, op);
       ti = A::scale(ti, op);
       if constexpr (MODE == kCheb) {
@@ -667,12 +782,12 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
 // access is a wide load. Same arithmetic per element as k_step; with FastArith the
 // moment uses the FP64 value of T_m before its FP32 rounding and plain FP64 per-thread
 // sums (a few dozen terms each), merged with TwoSum across lanes, blocks and the grid.
-template <typename VT2, int V, int W, int Z, class A, int MODE, bool DOT>
+template <typename VT2, int V, int W, int Z, class A, int MODE, bool DOT, bool C>
 __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
                                                      const VT2* __restrict__ t1, VT2* out,
                                                      const VT2* __restrict__ left, Dot dot)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   constexpr int kTps = V / W;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
   const size_t items = (size_t)op.n * kTps;
@@ -680,8 +795,21 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
 #pragma unroll
   for (int k = 0; k < W; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
-  // One item: W consecutive vectors of one site; `row` adds the neighbour terms.
-  auto item = [&](size_t g, auto&& row) {
+  // Pipelined as in k_step where the policy says so: the next item's row first.
+  constexpr bool kPre = Z > 0 && pipelined<kPipeStepVec, C, VT2, Z>();
+  RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
+  const size_t stride = (size_t)gridDim.x * kBlock;
+  size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
+  if constexpr (kPre) {
+    if (g < items)
+      fetch_row<(Z > 0 ? Z : 1), C>(op, (int)(g / kTps), cur);
+  }
+  for (; g < items; g += stride) {
+    if constexpr (kPre) {
+      nxt = cur;
+      if (g + stride < items)
+        fetch_row<(Z > 0 ? Z : 1), C>(op, (int)((g + stride) / kTps), nxt);
+    }
     const int i = (int)(g / kTps);
     const int v0 = (int)(g % kTps) * W;
     const size_t base = (size_t)i * V + v0;
@@ -694,7 +822,33 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
       tr[k] = A::mul(p, x[k].x);
       ti[k] = A::mul(p, x[k].y);
     }
-    row(i, v0, tr, ti);
+    if constexpr (kPre) {
+      hop_row_w<V, W, (Z > 0 ? Z : 1), A, C>(op, tb, i, v0, cur, t1, tr, ti);
+    } else {
+      const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+      auto body = [&](int m) {
+        const size_t e = (size_t)m * op.n + i;
+        int j, c;
+        double2 h;
+        ell_entry<C>(op, tb, e, i, j, h, c);
+        double2 y[W];
+        ldw<W>(t1 + (size_t)j * V + v0, y);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+          ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+        }
+      };
+      if constexpr (Z > 0) {
+#pragma unroll
+        for (int m = 0; m < Z; ++m)
+          if (m < cnt)
+            body(m);
+      } else {
+        for (int m = 0; m < cnt; ++m)
+          body(m);
+      }
+    }
     double2 r[W];
     if constexpr (MODE == kCheb) {
       double2 y0[W];
@@ -722,42 +876,8 @@ __global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
         }
       }
     }
-  };
-  const size_t stride = (size_t)gridDim.x * kBlock;
-  size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
-  if constexpr (Z > 0 && GQT_STEP_PREFETCH > 0) {
-    // Software-pipelined as in k_step: the next item's row is loaded first.
-    RowIdx<Z> cur;
-    if (g < items)
-      fetch_row<Z>(op, tb, (int)(g / kTps), cur);
-    for (; g < items; g += stride) {
-      RowIdx<Z> nxt = cur;
-      if (g + stride < items)
-        fetch_row<Z>(op, tb, (int)((g + stride) / kTps), nxt);
-      item(g, [&](int i, int v0, double(&tr)[W], double(&ti)[W]) {
-        hop_row_w<V, W, Z, A>(op, tb, i, v0, cur, t1, tr, ti);
-      });
+    if constexpr (kPre)
       cur = nxt;
-    }
-  } else {
-    for (; g < items; g += stride) {
-      item(g, [&](int i, int v0, double(&tr)[W], double(&ti)[W]) {
-        const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
-        for (int m = 0; m < cnt; ++m) {
-          const size_t e = (size_t)m * op.n + i;
-          int j, c;
-          double2 h;
-          ell_entry(op, tb, e, i, j, h, c);
-          double2 y[W];
-          ldw<W>(t1 + (size_t)j * V + v0, y);
-#pragma unroll
-          for (int k = 0; k < W; ++k) {
-            tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
-            ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
-          }
-        }
-      });
-    }
   }
   if constexpr (DOT)
     dot_finish_w<V, W>(re, im, dot);
@@ -826,12 +946,12 @@ __device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSu
 // sums are reduced over the block when the run ends and written to the block's slot
 // of that realisation; slots of realisations it never meets are zeroed.
 // k_tile_reduce then sums the blocks per realisation in fixed order.
-template <typename VT2, int V, int W, int Z, class A, int MODE>
+template <typename VT2, int V, int W, int Z, class A, int MODE, bool C>
 __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
                                                        const VT2* __restrict__ left, MultiDot md)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   constexpr int kTps = V / W;
   constexpr int kWarps = kBlock / 32;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
@@ -872,18 +992,18 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
     }
     any = true;
     // Software-pipelined within the tile: the next item's row is loaded first.
-    constexpr bool kPre = Z > 0 && GQT_STEP_PREFETCH > 0 && MODE != kDotOnly;
+    constexpr bool kPre = Z > 0 && pipelined<kPipeStepMulti, C, VT2, Z>() && MODE != kDotOnly;
     RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
     if constexpr (kPre) {
       if (threadIdx.x < items_per_tile)
-        fetch_row(op, tb, (int)(((size_t)t * items_per_tile + threadIdx.x) / kTps), cur);
+        fetch_row<(Z > 0 ? Z : 1), C>(op, (int)(((size_t)t * items_per_tile + threadIdx.x) / kTps), cur);
     }
     for (size_t it = threadIdx.x; it < items_per_tile; it += kBlock) {
       const size_t g = (size_t)t * items_per_tile + it;
       if constexpr (kPre) {
         nxt = cur;
         if (it + kBlock < items_per_tile)
-          fetch_row(op, tb, (int)((g + kBlock) / kTps), nxt);
+          fetch_row<(Z > 0 ? Z : 1), C>(op, (int)((g + kBlock) / kTps), nxt);
       }
       const int i = (int)(g / kTps);
       const int v0 = (int)(g % kTps) * W;
@@ -902,14 +1022,14 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
           ti[k] = A::mul(p, x[k].y);
         }
         if constexpr (kPre) {
-          hop_row_w<V, W, (Z > 0 ? Z : 1), A>(op, tb, i, v0, cur, t1, tr, ti);
+          hop_row_w<V, W, (Z > 0 ? Z : 1), A, C>(op, tb, i, v0, cur, t1, tr, ti);
         } else {
           const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
-          for (int m = 0; m < cnt; ++m) {
+          auto body = [&](int m) {
             const size_t e = (size_t)m * op.n + i;
             int j, c;
             double2 h;
-            ell_entry(op, tb, e, i, j, h, c);
+            ell_entry<C>(op, tb, e, i, j, h, c);
             double2 y[W];
             ldw<W>(t1 + (size_t)j * V + v0, y);
 #pragma unroll
@@ -917,6 +1037,15 @@ __global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
               tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
               ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
             }
+          };
+          if constexpr (Z > 0) {
+#pragma unroll
+            for (int m = 0; m < Z; ++m)
+              if (m < cnt)
+                body(m);
+          } else {
+            for (int m = 0; m < cnt; ++m)
+              body(m);
           }
         }
         if constexpr (MODE == kCheb) {
@@ -997,11 +1126,11 @@ __global__ void __launch_bounds__(kBlock) k_tile_reduce(MultiDot md)
 
 // [X,H] in / E_max (src/hamiltonian.cu:240-271) or V in = -i sum H xx in
 // (src/hamiltonian.cu:323-352).
-template <typename VT2, int V, int Z, class A, bool CURRENT>
+template <typename VT2, int V, int Z, class A, bool CURRENT, bool C>
 __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ in,
                                                 VT2* __restrict__ out)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   const size_t total = (size_t)op.n * V;
   auto term = [&](double& tr, double& ti, double2 h, double2 y, double x) {
     if constexpr (CURRENT) {
@@ -1019,8 +1148,8 @@ __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ i
       st(out + g, make_double2(A::scale(tr, op), A::scale(ti, op)));
     }
   };
-  if constexpr (Z > 0) {
-    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+  if constexpr (Z > 0 && pipelined<kPipeXop, C, VT2, Z>()) {
+    pipelined_rows<Z, V, C>(op, total, [&](size_t g, const RowIdx<Z>& r) {
       const int i = (int)(g / V);
       const int v = (int)(g % V);
       double tr = 0.0, ti = 0.0;
@@ -1029,8 +1158,8 @@ __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ i
         if (m < r.cnt) {
           int j;
           double2 h;
-          row_entry(op, tb, i, m, r.idx[m], j, h);
-          term(tr, ti, h, ld(in + (size_t)j * V + v), row_xx(op, tb, i, m, r.idx[m]));
+          row_entry<C>(op, tb, i, m, r.idx[m], j, h);
+          term(tr, ti, h, ld(in + (size_t)j * V + v), row_xx<C>(op, tb, i, m, r.idx[m]));
         }
       }
       finish(g, tr, ti);
@@ -1042,13 +1171,13 @@ __global__ void __launch_bounds__(kBlock) k_xop(Op op, const VT2* __restrict__ i
       const int v = (int)(g % V);
       const int cnt = op.uniform ? op.z : op.nn[i];
       double tr = 0.0, ti = 0.0;
-      for (int m = 0; m < cnt; ++m) {
+      for_entries<Z>(cnt, [&](int m) {
         const size_t e = (size_t)m * op.n + i;
         int j, c;
         double2 h;
-        ell_entry(op, tb, e, i, j, h, c);
-        term(tr, ti, h, ld(in + (size_t)j * V + v), ell_xx(op, tb, e, c));
-      }
+        ell_entry<C>(op, tb, e, i, j, h, c);
+        term(tr, ti, h, ld(in + (size_t)j * V + v), ell_xx<C>(op, tb, e, c));
+      });
       finish(g, tr, ti);
     }
   }
@@ -1103,13 +1232,13 @@ __device__ __forceinline__ double2 accumulate(double2 o, double b, double tr, do
 
 // gpu_chebyshev_2 (src/hamiltonian.cu:465-529): s2 = 2 H s1 / E_max - s0 and
 // out += (label) * bessel * s2. s2 may alias s0.
-template <typename VT2, typename OT2, int V, int Z, class A>
+template <typename VT2, typename OT2, int V, int Z, class A, bool C>
 __global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
                                                   const VT2* __restrict__ s1, VT2* s2,
                                                   OT2* __restrict__ out, double bessel,
                                                   int label)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   const size_t total = (size_t)op.n * V;
   auto item = [&](size_t g, auto&& row) {
     const int i = (int)(g / V);
@@ -1126,17 +1255,17 @@ __global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
     st(out + g, accumulate<A>(ld(out + g), bessel, tr, ti, label));
     st(s2 + g, make_double2(tr, ti));
   };
-  if constexpr (Z > 0) {
-    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+  if constexpr (Z > 0 && pipelined<kPipeCheb2, C, VT2, Z>()) {
+    pipelined_rows<Z, V, C>(op, total, [&](size_t g, const RowIdx<Z>& r) {
       item(g, [&](int i, int v, double& tr, double& ti) {
-        hop_row_pre<V, Z, A>(op, tb, i, v, r, s1, tr, ti);
+        hop_row_pre<V, Z, A, C>(op, tb, i, v, r, s1, tr, ti);
       });
     });
   } else {
     for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
          g += (size_t)gridDim.x * kBlock)
       item(g, [&](int i, int v, double& tr, double& ti) {
-        hop_row<V, Z, A>(op, tb, i, v, s1, tr, ti);
+        hop_row<V, Z, A, C>(op, tb, i, v, s1, tr, ti);
       });
   }
 }
@@ -1144,14 +1273,14 @@ __global__ void __launch_bounds__(kBlock) k_cheb2(Op op, const VT2* s0,
 // gpu_chebyshev_2x (src/hamiltonian.cu:666-758): the coupled recurrences of T_m and
 // [X, T_m], accumulating out += (label) * bessel * [X, T_m]. s2 may alias s0 and s2x
 // may alias s0x.
-template <typename VT2, typename OT2, int V, int Z, class A>
+template <typename VT2, typename OT2, int V, int Z, class A, bool C>
 __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const VT2* s0x,
                                                    const VT2* __restrict__ s1,
                                                    const VT2* __restrict__ s1x, VT2* s2,
                                                    VT2* s2x, OT2* __restrict__ out,
                                                    double bessel, int label)
 {
-  const Tables tb = load_tables(op);
+  const Tables tb = load_tables<C>(op);
   const size_t total = (size_t)op.n * V;
   auto item = [&](size_t g, auto&& row) {
     const int i = (int)(g / V);
@@ -1181,17 +1310,17 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
     st(s2x + g, make_double2(txr, txi));
     st(out + g, accumulate<A>(ld(out + g), bessel, txr, txi, label));
   };
-  if constexpr (Z > 0) {
-    pipelined_rows<Z, V>(op, tb, total, [&](size_t g, const RowIdx<Z>& r) {
+  if constexpr (Z > 0 && pipelined<kPipeCheb2x, C, VT2, Z>()) {
+    pipelined_rows<Z, V, C>(op, total, [&](size_t g, const RowIdx<Z>& r) {
       item(g, [&](int i, int v, auto&& term) {
 #pragma unroll
         for (int m = 0; m < Z; ++m) {
           if (m < r.cnt) {
             int j;
             double2 h;
-            row_entry(op, tb, i, m, r.idx[m], j, h);
+            row_entry<C>(op, tb, i, m, r.idx[m], j, h);
             term(h, ld(s1 + (size_t)j * V + v), ld(s1x + (size_t)j * V + v),
-                 row_xx(op, tb, i, m, r.idx[m]));
+                 row_xx<C>(op, tb, i, m, r.idx[m]));
           }
         }
       });
@@ -1201,13 +1330,13 @@ __global__ void __launch_bounds__(kBlock) k_cheb2x(Op op, const VT2* s0, const V
          g += (size_t)gridDim.x * kBlock)
       item(g, [&](int i, int v, auto&& term) {
         const int cnt = op.uniform ? op.z : op.nn[i];
-        for (int m = 0; m < cnt; ++m) {
+        for_entries<Z>(cnt, [&](int m) {
           const size_t e = (size_t)m * op.n + i;
           int j, c;
           double2 h;
-          ell_entry(op, tb, e, i, j, h, c);
-          term(h, ld(s1 + (size_t)j * V + v), ld(s1x + (size_t)j * V + v), ell_xx(op, tb, e, c));
-        }
+          ell_entry<C>(op, tb, e, i, j, h, c);
+          term(h, ld(s1 + (size_t)j * V + v), ld(s1x + (size_t)j * V + v), ell_xx<C>(op, tb, e, c));
+        });
       });
   }
 }

@@ -38,7 +38,7 @@ int z_index(int z) { return z == 3 ? 0 : z == 4 ? 1 : z == 6 ? 2 : 3; }
 template <int V, int Z, int MODE>
 const void* kernel_of()
 {
-  return (const void*)gqt::k_step<double2, V, Z, ExactArith, MODE, true>;
+  return (const void*)gqt::k_step<double2, V, Z, ExactArith, MODE, true, false>;
 }
 
 template <int V, int MODE>
@@ -105,19 +105,19 @@ void launch(int grid, cudaStream_t s, const Op& op, const double2* t0, const dou
 {
   switch (z_index(op.z)) {
     case 0:
-      gqt::k_step<double2, V, 3, ExactArith, MODE, true><<<grid, kBlock, 0, s>>>(op, t0, t1,
+      gqt::k_step<double2, V, 3, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
                                                                                  out, left, d);
       break;
     case 1:
-      gqt::k_step<double2, V, 4, ExactArith, MODE, true><<<grid, kBlock, 0, s>>>(op, t0, t1,
+      gqt::k_step<double2, V, 4, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
                                                                                  out, left, d);
       break;
     case 2:
-      gqt::k_step<double2, V, 6, ExactArith, MODE, true><<<grid, kBlock, 0, s>>>(op, t0, t1,
+      gqt::k_step<double2, V, 6, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
                                                                                  out, left, d);
       break;
     default:
-      gqt::k_step<double2, V, 0, ExactArith, MODE, true><<<grid, kBlock, 0, s>>>(op, t0, t1,
+      gqt::k_step<double2, V, 0, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
                                                                                  out, left, d);
       break;
   }
