@@ -4,14 +4,16 @@
 One step = one KPM moment set: mu_m = <phi|T_m(H/E_max)|phi>, m < 3000, over the
 honeycomb graphene lattice of 2,097,152 sites (4-orbital cell x 1024x512, t = -2.7 eV,
 Anderson W = 1.0 eV, seed 3, E_max 8.7 eV) for one random-phase vector per GPU, in the
-plain FP64 form (the reference's arithmetic). value = site-moments/s over all ranks
-(sites x moments x steps / max-over-ranks device time).
+plain FP64 form (the reference's arithmetic, bit-identical per site) with the operator
+in its default device format (coded: one byte per ELL entry). value = site-moments/s
+over all ranks (sites x moments x steps / max-over-ranks device time).
 
 Also reported: the roofline of the dominant kernel (the fused Chebyshev step + moment
 partial sums), the same metric end to end through the public API with host buffers
-(e2e), the FP32-storage batched form (16 vectors per launch) with its DOS error
-against FP64, the Bessel evolution cost, and the reference's CPU path timed on this
-host's cores (cpu_baseline).
+(e2e), the plain FP64 rate on the reference's ELL arrays, the FP32-storage batched
+form (16 vectors per launch) with its DOS error against FP64 and its speed-up over
+both FP64 rates, the realisation batch, the Bessel evolution cost, and the
+reference's CPU path timed on this host's cores (cpu_baseline).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU runs are launched with torchrun, one rank per GPU (independent replicas).
