@@ -115,6 +115,8 @@ _SIGS = {
     "gqt_model_time_step": (ctypes.c_int, [_vp, _dp]),
     "gqt_model_initial_state": (ctypes.c_int, [_vp, ctypes.c_int, _dp, _dp]),
     "gqt_lsqt": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int]),
+    "gqt_lsqt_run": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_int, ctypes.c_int,
+                                    ctypes.c_longlong, _ip]),
     "gqt_chebyshev_step_noalloc": (ctypes.c_int, [_vp, ctypes.c_int, _vp, _vp, _vp, _vp, _vp]),
 }
 
@@ -519,6 +521,30 @@ def chebyshev_summation(mu_re, mu_im, energy, energy_max: float, volume: float):
     return out
 
 
-def lsqt(input_dir: str, precision: int = FP64, verbose: bool = False) -> None:
-    """The full run of one input directory (lsqt, src/lsqt.cu:135-152)."""
-    _call("gqt_lsqt", input_dir.encode(), precision, int(verbose))
+def lsqt(input_dir: str, precision: int = FP64, verbose: bool = False,
+         max_rows: int = 0) -> bool:
+    """The full run of one input directory (lsqt, src/lsqt.cu:135-152). With
+    max_rows > 0 the run stops after that many .out rows, leaving a checkpoint that
+    the next call resumes (gqt_lsqt_run); returns whether the run is complete."""
+    done = ctypes.c_int()
+    _call("gqt_lsqt_run", input_dir.encode(), precision, int(verbose), int(max_rows),
+          ctypes.byref(done))
+    return bool(done.value)
+
+
+MOMENTS_MAGIC = b"GQTMOMv1"
+
+
+def read_moments(path: str):
+    """Raw moments written with para.in `output_moments`: (re, im), each of shape
+    (rows, number_of_moments), one row per .out row in the same order."""
+    with open(path, "rb") as f:
+        head = f.read(16)
+        if len(head) != 16 or head[:8] != MOMENTS_MAGIC:
+            raise ValueError(f"{path}: not a moments file")
+        m = int(np.frombuffer(head[8:12], dtype="<i4")[0])
+        data = np.frombuffer(f.read(), dtype="<f8")
+    if m <= 0 or data.size % (2 * m):
+        raise ValueError(f"{path}: size is not a whole number of rows")
+    rows = data.reshape(-1, m, 2)
+    return rows[:, :, 0].copy(), rows[:, :, 1].copy()

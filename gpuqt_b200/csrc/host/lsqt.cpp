@@ -2,7 +2,11 @@
 // model / driver entry points (gqt_model_*, gqt_lsqt).
 #include "lsqt/lsqt.h"
 
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <chrono>
+#include <cstdio>
 #include <cstring>
 #include <iostream>
 #include <vector>
@@ -12,6 +16,8 @@
 #include "lsqt/model.h"
 #include "lsqt/sigma.h"
 #include "lsqt/vector.h"
+#include "checkpoint.h"
+#include "stages.h"
 
 namespace {
 
@@ -27,35 +33,193 @@ void timed(bool verbose, const char* what, F&& f)
     std::cout << "- Time used for finding " << what << " = " << s << " s" << std::endl;
 }
 
-void run(Model& model)
+// The row budget of a bounded run is spent (a checkpoint has been written).
+struct StopRun {};
+
+using gqt_host::RunPosition;
+
+bool stage_on(const Model& m, int stage)
 {
+  switch (stage) {
+    case gqt_host::kStageDos:
+      return true;
+    case gqt_host::kStageVac0:
+      return m.calculate_vac0;
+    case gqt_host::kStageVac:
+      return m.calculate_vac;
+    case gqt_host::kStageMsd:
+      return m.calculate_msd;
+    case gqt_host::kStageSpin:
+      return m.calculate_spin;
+    case gqt_host::kStageLdos:
+      return m.calculate_ldos;
+    default:
+      return false;
+  }
+}
+
+int stage_rows(const Model& m, int stage)
+{
+  if (stage == gqt_host::kStageDos || stage == gqt_host::kStageVac0)
+    return 1;
+  if (stage == gqt_host::kStageLdos)
+    return m.number_of_local_orbitals;
+  return m.number_of_steps_correlation;
+}
+
+// Where the run continues after the row that left `stage` of `vector` at `next`.
+RunPosition next_position(const Model& m, int vector, int stage, int next)
+{
+  if (next < stage_rows(m, stage))
+    return {vector, stage, next};
+  if (stage < gqt_host::kStageLdos) {
+    for (int s = stage + 1; s < gqt_host::kStageLdos; ++s)
+      if (stage_on(m, s))
+        return {vector, s, 0};
+    if (vector + 1 < m.number_of_random_vectors)
+      return {vector + 1, gqt_host::kStageDos, 0};
+  }
+  const int v = m.number_of_random_vectors;
+  if (stage < gqt_host::kStageLdos && stage_on(m, gqt_host::kStageLdos) &&
+      m.number_of_local_orbitals > 0)
+    return {v, gqt_host::kStageLdos, 0};
+  return {v, gqt_host::kStageEnd, 0};
+}
+
+uint64_t file_size(const std::string& path)
+{
+  struct stat st;
+  return stat(path.c_str(), &st) == 0 ? (uint64_t)st.st_size : 0;
+}
+
+// The run over one input directory. Checkpointing is on when para.in asks for it
+// (checkpoint_every) or the run is bounded (max_rows > 0): an existing checkpoint is
+// then resumed, one is written every checkpoint_every rows and when the row budget is
+// spent (StopRun), and it is removed when the run completes. With checkpointing off
+// this is the reference's run, row for row.
+void run(Model& model, long long max_rows, int precision)
+{
+  using namespace gqt_host;
+  const bool ckpt = model.checkpoint_every > 0 || max_rows > 0;
+  const std::string path = checkpoint_path(model);
+  Checkpoint ck;
+  RunPosition start;
+  bool resumed = false;
+  uint64_t fingerprint = 0;
+  if (ckpt) {
+    fingerprint = run_fingerprint(model, precision);  // before the Hamiltonian takes the arrays
+    if (load_checkpoint(path, ck)) {
+      if (ck.fingerprint != fingerprint)
+        throw InputError(path + " belongs to a different run (parameters, operator or precision changed)");
+      for (size_t k = 0; k < ck.files.size(); ++k) {
+        const std::string f = model.input_dir + "/" + ck.files[k];
+        const uint64_t have = file_size(f);
+        if (have < ck.sizes[k])
+          throw InputError(f + " is shorter than at the checkpoint; cannot resume");
+        if (have > ck.sizes[k] && truncate(f.c_str(), (off_t)ck.sizes[k]) != 0)
+          die("Error: cannot truncate " + f, GQT_ERR_IO);
+      }
+      model.set_rng_state(ck.rng);
+      start = ck.pos;
+      resumed = true;
+      if (model.verbose)
+        std::cout << "Resuming from " << path << " at random vector " << start.vector
+                  << ", stage " << start.stage << ", step " << start.step << std::endl;
+    }
+  }
+
   Hamiltonian H(model);
   Vector random_state(model.number_of_atoms);
   const bool v = model.verbose;
-  for (int i = 0; i < model.number_of_random_vectors; ++i) {
+  long long rows = 0;
+  int since = 0;
+  std::string rng_before;  // the generator before the current vector's phase draw
+  int current = -1;        // the vector being run
+  auto save = [&](const RunPosition& pos, const std::vector<Vector*>& live) {
+    Checkpoint c;
+    c.fingerprint = fingerprint;
+    c.pos = pos;
+    c.rng = pos.vector == current ? rng_before : model.rng_state();
+    c.files = output_files(model);
+    for (const auto& f : c.files)
+      c.sizes.push_back(file_size(model.input_dir + "/" + f));
+    const size_t n = (size_t)model.number_of_atoms;
+    for (Vector* s : live) {
+      std::vector<real> buf(2 * n);
+      s->copy_to_host(buf.data(), buf.data() + n);
+      c.states.push_back(std::move(buf));
+    }
+    save_checkpoint(path, c);
+    since = 0;
+  };
+  auto after_row = [&](const RunPosition& pos, const std::vector<Vector*>& live) {
+    ++rows;
+    ++since;
+    if (!ckpt)
+      return;
+    const bool stop = max_rows > 0 && rows >= max_rows;
+    if (stop || (model.checkpoint_every > 0 && since >= model.checkpoint_every))
+      save(pos, live);
+    if (stop)
+      throw StopRun{};
+  };
+  auto stage_run = [&](int vector, int stage, StageRun& sr) {
+    const bool first = resumed && vector == start.vector && stage == start.stage;
+    sr.start = first ? start.step : 0;
+    sr.restore = first ? &ck.states : nullptr;
+    sr.after_row = [&, vector, stage](int next, const std::vector<Vector*>& live) {
+      after_row(next_position(model, vector, stage, next), live);
+    };
+  };
+
+  const int first_vector = resumed ? start.vector : 0;
+  for (int i = first_vector; i < model.number_of_random_vectors; ++i) {
     if (v)
       std::cout << "\nStarted  simulation with random vector number " << i << std::endl;
+    current = i;
+    rng_before = model.rng_state();
     model.initialize_state(random_state, -1);
-    timed(v, "DOS", [&] { find_dos(model, H, random_state, 0); });
-    if (model.calculate_vac0)
-      timed(v, "VAC0", [&] { find_vac0(model, H, random_state); });
-    if (model.calculate_vac)
-      timed(v, "VAC", [&] { find_vac(model, H, random_state); });
-    if (model.calculate_msd)
-      timed(v, "MSD", [&] { find_msd(model, H, random_state); });
-    if (model.calculate_spin)
-      timed(v, "spin polarization", [&] { find_spin_polarization(model, H, random_state); });
+    const int first_stage = (resumed && i == start.vector) ? start.stage : kStageDos;
+    StageRun sr;
+    if (first_stage <= kStageDos) {
+      stage_run(i, kStageDos, sr);
+      timed(v, "DOS", [&] { dos_stage(model, H, random_state, 0, sr); });
+    }
+    if (model.calculate_vac0 && first_stage <= kStageVac0) {
+      stage_run(i, kStageVac0, sr);
+      timed(v, "VAC0", [&] { vac0_stage(model, H, random_state, sr); });
+    }
+    if (model.calculate_vac && first_stage <= kStageVac) {
+      stage_run(i, kStageVac, sr);
+      timed(v, "VAC", [&] { vac_stage(model, H, random_state, sr); });
+    }
+    if (model.calculate_msd && first_stage <= kStageMsd) {
+      stage_run(i, kStageMsd, sr);
+      timed(v, "MSD", [&] { msd_stage(model, H, random_state, sr); });
+    }
+    if (model.calculate_spin && first_stage <= kStageSpin) {
+      stage_run(i, kStageSpin, sr);
+      timed(v, "spin polarization", [&] { spin_stage(model, H, random_state, sr); });
+    }
     if (v)
       std::cout << "Finished simulation with random vector number " << i << std::endl;
   }
-  if (model.calculate_ldos) {
+  current = -1;
+  if (model.calculate_ldos && !(resumed && start.stage == kStageEnd)) {
+    const int k0 = (resumed && start.stage == kStageLdos) ? start.step : 0;
     timed(v, "LDOS", [&] {
-      for (int i = 0; i < model.number_of_local_orbitals; ++i) {
-        model.initialize_state(random_state, model.local_orbitals[i]);
-        find_dos(model, H, random_state, 1);
+      for (int k = k0; k < model.number_of_local_orbitals; ++k) {
+        model.initialize_state(random_state, model.local_orbitals[k]);
+        StageRun sr;
+        sr.after_row = [&, k](int, const std::vector<Vector*>&) {
+          after_row(next_position(model, model.number_of_random_vectors, kStageLdos, k + 1), {});
+        };
+        dos_stage(model, H, random_state, 1, sr);
       }
     });
   }
+  if (ckpt)
+    std::remove(path.c_str());
 }
 
 }  // namespace
@@ -63,7 +227,11 @@ void run(Model& model)
 void lsqt(std::string input_directory)
 {
   Model model(input_directory);
-  run(model);
+  try {
+    run(model, 0, Vector::moment_precision);
+  } catch (const gqt_host::InputError& e) {
+    gqt_host::die(std::string("Error: ") + e.what());
+  }
 }
 
 // ------------------------------------------------------------------ C ABI
@@ -161,8 +329,11 @@ extern "C" gqt_status gqt_model_initial_state(gqt_model* gm, int orbital, double
   return GQT_OK;
 }
 
-extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
+extern "C" gqt_status gqt_lsqt_run(const char* dir, int precision, int verbose,
+                                   long long max_rows, int* finished)
 {
+  if (finished)
+    *finished = 0;
   if (!dir)
     return GQT_ERR_ARG;
   if (precision != GQT_FP64 && precision != GQT_FP32)
@@ -174,7 +345,11 @@ extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
   try {
     Model model(dir, Model::Quiet{});
     model.verbose = verbose != 0;
-    run(model);
+    run(model, max_rows, precision);
+    if (finished)
+      *finished = 1;
+  } catch (const StopRun&) {
+    // the row budget is spent; the checkpoint holds the rest of the run
   } catch (const gqt_host::InputError& e) {
     gqt_host::set_error(e.what());
     st = GQT_ERR_INPUT;
@@ -184,4 +359,9 @@ extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
   }
   Vector::moment_precision = saved;
   return st;
+}
+
+extern "C" gqt_status gqt_lsqt(const char* dir, int precision, int verbose)
+{
+  return gqt_lsqt_run(dir, precision, verbose, 0, nullptr);
 }

@@ -147,12 +147,18 @@ void Model::initialize_parameters()
       ss >> disorder_seed;
     } else if (token == "phase_seed") {
       ss >> phase_seed;
+    } else if (token == "output_moments") {
+      output_moments = true;
+    } else if (token == "checkpoint_every") {
+      ss >> checkpoint_every;
+      if (!ss || checkpoint_every < 1)
+        bad("checkpoint_every needs a number of rows >= 1");
     } else {
       bad("Unknown identifier in " + filename + ": " + line +
           "\nValid keywords include: model anderson_disorder charged_impurity "
           "vacancy_disorder calculate_vac0 calculate_vac calculate_msd calculate_spin "
           "calculate_ldos number_of_random_vectors number_of_moments energy_max seed "
-          "disorder_seed phase_seed");
+          "disorder_seed phase_seed output_moments checkpoint_every");
     }
   }
   verify_parameters();
@@ -704,6 +710,23 @@ void Model::initialize_state_host(real* re, real* im, int orbital)
       im[n] = std::sin(p);
     }
   }
+}
+
+std::string Model::rng_state() const
+{
+  std::ostringstream os;
+  os << (phase_reseeded ? 1 : 0) << ' ' << generator;
+  return os.str();
+}
+
+void Model::set_rng_state(const std::string& state)
+{
+  std::istringstream is(state);
+  int reseeded = 0;
+  is >> reseeded >> generator;
+  if (!is)
+    bad("the checkpoint's generator state cannot be read");
+  phase_reseeded = reseeded != 0;
 }
 
 void Model::initialize_state(Vector& random_state, int orbital)

@@ -12,6 +12,8 @@
 #include "lsqt/hamiltonian.h"
 #include "lsqt/model.h"
 #include "lsqt/vector.h"
+#include "checkpoint.h"
+#include "stages.h"
 
 using gqt_host::check;
 
@@ -78,119 +80,198 @@ void evolvex(Model&, int direction, real time_step_scaled, Hamiltonian& H, Vecto
 
 namespace {
 
-// Moments -> damped Chebyshev sum -> one appended row of `file`.
-void write_row(Model& model, Vector& moments, const std::string& file, std::ofstream& out)
+// Moments -> damped Chebyshev sum -> one appended row of <stem>.out; with
+// output_moments, the raw moments also go to <stem>_moments.bin.
+void write_row(Model& model, Vector& moments, const char* stem, std::ofstream& out)
 {
   const int M = model.number_of_moments;
   std::vector<real> re(M), im(M), row(model.number_of_energy_points);
   moments.copy_to_host(re.data(), im.data());
+  if (model.output_moments)
+    gqt_host::append_moments(model.input_dir + "/" + stem + "_moments.bin", M, re.data(),
+                             im.data());
   apply_damping(model, re.data(), im.data());
   perform_chebyshev_summation(model, re.data(), im.data(), row.data());
   for (int n = 0; n < model.number_of_energy_points; ++n)
     out << row[n] << " ";
   out << std::endl;
   if (!out)
-    gqt_host::die("Error: cannot write " + file);
+    gqt_host::die("Error: cannot write " + model.input_dir + "/" + stem + ".out");
 }
 
-std::ofstream open_out(Model& model, const char* name)
+std::ofstream open_out(Model& model, const char* stem)
 {
-  const std::string file = model.input_dir + name;
+  const std::string file = model.input_dir + "/" + stem + ".out";
   std::ofstream out(file, std::ios::app);
   if (!out.is_open())
     gqt_host::die("Error: cannot open " + file);
   return out;
 }
 
+void restore(Vector& v, const std::vector<real>& s)
+{
+  const size_t n = (size_t)v.size();
+  if (s.size() != 2 * n)
+    gqt_host::die("Error: a checkpointed state does not match the model size", GQT_ERR_INPUT);
+  std::vector<real> re(s.begin(), s.begin() + n), im(s.begin() + n, s.end());
+  v.copy_from_host(re.data(), im.data());
+}
+
+void report(gqt_host::StageRun& run, int next, std::vector<Vector*> live)
+{
+  if (run.after_row)
+    run.after_row(next, live);
+}
+
 }  // namespace
 
+namespace gqt_host {
+
 // src/sigma.cu:204-239.
-void find_dos(Model& model, Hamiltonian& H, Vector& random_state, int flag)
+void dos_stage(Model& model, Hamiltonian& H, Vector& random_state, int flag, StageRun& run)
 {
   Vector moments(model.number_of_moments, GQT_FP64);
   find_moments_chebyshev(model, H, random_state, random_state, moments);
-  const char* name = flag == 0 ? "/dos.out" : "/ldos.out";
-  std::ofstream out = open_out(model, name);
-  write_row(model, moments, model.input_dir + name, out);
+  const char* stem = flag == 0 ? "dos" : "ldos";
+  std::ofstream out = open_out(model, stem);
+  write_row(model, moments, stem, out);
+  report(run, 1, {});
 }
 
 // src/sigma.cu:243-274.
-void find_vac0(Model& model, Hamiltonian& H, Vector& random_state)
+void vac0_stage(Model& model, Hamiltonian& H, Vector& random_state, StageRun& run)
 {
   Vector moments(model.number_of_moments, GQT_FP64);
   Vector state(model.number_of_atoms);
   H.apply_current(random_state, state);
   find_moments_chebyshev(model, H, state, state, moments);
-  std::ofstream out = open_out(model, "/vac0.out");
-  write_row(model, moments, model.input_dir + "/vac0.out", out);
+  std::ofstream out = open_out(model, "vac0");
+  write_row(model, moments, "vac0", out);
+  report(run, 1, {});
 }
 
 // src/sigma.cu:278-327.
-void find_vac(Model& model, Hamiltonian& H, Vector& random_state)
+void vac_stage(Model& model, Hamiltonian& H, Vector& random_state, StageRun& run)
 {
   Vector state_left(random_state);
   Vector state_left_copy(model.number_of_atoms);
   Vector state_right(random_state);
   Vector moments(model.number_of_moments, GQT_FP64);
-  H.apply_current(state_left, state_right);
-  std::ofstream out = open_out(model, "/vac.out");
-  for (int m = 0; m < model.number_of_steps_correlation; ++m) {
+  if (run.start > 0) {
+    restore(state_left, run.restore->at(0));
+    restore(state_right, run.restore->at(1));
+  } else {
+    H.apply_current(state_left, state_right);
+  }
+  std::ofstream out = open_out(model, "vac");
+  const int steps = model.number_of_steps_correlation;
+  for (int m = run.start; m < steps; ++m) {
     if (model.verbose)
       std::cout << "- calculating VAC step " << m << std::endl;
     H.apply_current(state_left, state_left_copy);
     find_moments_chebyshev(model, H, state_right, state_left_copy, moments);
-    write_row(model, moments, model.input_dir + "/vac.out", out);
-    if (m < model.number_of_steps_correlation - 1) {
+    write_row(model, moments, "vac", out);
+    if (m < steps - 1) {
       const real dt = model.time_step[m] * model.energy_max;
       evolve(model, -1, dt, H, state_left);
       evolve(model, -1, dt, H, state_right);
+      report(run, m + 1, {&state_left, &state_right});
+    } else {
+      report(run, steps, {});
     }
   }
 }
 
 // src/sigma.cu:331-391 (note the time step index m + 1 inside the loop).
-void find_msd(Model& model, Hamiltonian& H, Vector& random_state)
+void msd_stage(Model& model, Hamiltonian& H, Vector& random_state, StageRun& run)
 {
   Vector state(random_state);
   Vector state_x(random_state);
   Vector state_copy(model.number_of_atoms);
   Vector moments(model.number_of_moments, GQT_FP64);
-  real dt = model.time_step[0] * model.energy_max;
-  evolve(model, 1, dt, H, state);
-  evolvex(model, 1, dt, H, state_x);
-  std::ofstream out = open_out(model, "/msd.out");
-  for (int m = 0; m < model.number_of_steps_correlation; ++m) {
+  if (run.start > 0) {
+    restore(state, run.restore->at(0));
+    restore(state_x, run.restore->at(1));
+  } else {
+    const real dt = model.time_step[0] * model.energy_max;
+    evolve(model, 1, dt, H, state);
+    evolvex(model, 1, dt, H, state_x);
+  }
+  std::ofstream out = open_out(model, "msd");
+  const int steps = model.number_of_steps_correlation;
+  for (int m = run.start; m < steps; ++m) {
     if (model.verbose)
       std::cout << "- calculating MSD step " << m << std::endl;
     find_moments_chebyshev(model, H, state_x, state_x, moments);
-    write_row(model, moments, model.input_dir + "/msd.out", out);
-    if (m < model.number_of_steps_correlation - 1) {
-      dt = model.time_step[m + 1] * model.energy_max;
+    write_row(model, moments, "msd", out);
+    if (m < steps - 1) {
+      const real dt = model.time_step[m + 1] * model.energy_max;
       state_copy.copy(state);
       evolvex(model, 1, dt, H, state_copy);
       evolve(model, 1, dt, H, state_x);
       state_x.add(state_copy);
       evolve(model, 1, dt, H, state);
+      report(run, m + 1, {&state, &state_x});
+    } else {
+      report(run, steps, {});
     }
   }
 }
 
 // src/sigma.cu:395-442.
-void find_spin_polarization(Model& model, Hamiltonian& H, Vector& random_state)
+void spin_stage(Model& model, Hamiltonian& H, Vector& random_state, StageRun& run)
 {
   Vector state(random_state);
   Vector state_sz(model.number_of_atoms);
   Vector moments(model.number_of_moments, GQT_FP64);
-  std::ofstream out = open_out(model, "/S.out");
-  for (int m = 0; m < model.number_of_steps_correlation; ++m) {
+  if (run.start > 0)
+    restore(state, run.restore->at(0));
+  std::ofstream out = open_out(model, "S");
+  const int steps = model.number_of_steps_correlation;
+  for (int m = run.start; m < steps; ++m) {
     if (model.verbose)
       std::cout << "- calculating spin step " << m << std::endl;
     state_sz.apply_sz(state);
     find_moments_chebyshev(model, H, state, state_sz, moments);
-    write_row(model, moments, model.input_dir + "/S.out", out);
-    if (m < model.number_of_steps_correlation - 1) {
+    write_row(model, moments, "S", out);
+    if (m < steps - 1) {
       const real dt = model.time_step[m] * model.energy_max;
       evolve(model, 1, dt, H, state);
+      report(run, m + 1, {&state});
+    } else {
+      report(run, steps, {});
     }
   }
+}
+
+}  // namespace gqt_host
+
+void find_dos(Model& model, Hamiltonian& H, Vector& random_state, int flag)
+{
+  gqt_host::StageRun run;
+  gqt_host::dos_stage(model, H, random_state, flag, run);
+}
+
+void find_vac0(Model& model, Hamiltonian& H, Vector& random_state)
+{
+  gqt_host::StageRun run;
+  gqt_host::vac0_stage(model, H, random_state, run);
+}
+
+void find_vac(Model& model, Hamiltonian& H, Vector& random_state)
+{
+  gqt_host::StageRun run;
+  gqt_host::vac_stage(model, H, random_state, run);
+}
+
+void find_msd(Model& model, Hamiltonian& H, Vector& random_state)
+{
+  gqt_host::StageRun run;
+  gqt_host::msd_stage(model, H, random_state, run);
+}
+
+void find_spin_polarization(Model& model, Hamiltonian& H, Vector& random_state)
+{
+  gqt_host::StageRun run;
+  gqt_host::spin_stage(model, H, random_state, run);
 }

@@ -262,6 +262,19 @@ gqt_status gqt_model_initial_state(gqt_model* m, int orbital, double* re, double
  * with the reference's formats. precision selects the arithmetic form of the moment
  * recurrence; states and their time evolution stay FP64. */
 gqt_status gqt_lsqt(const char* input_dir, int precision, int verbose);
+/* gqt_lsqt with checkpoint / resume; no counterpart in the reference. A checkpoint
+ * (input_dir/lsqt.checkpoint: the next row's position, the generator state, the
+ * evolved states and the output file sizes) is resumed when present and written
+ * every `checkpoint_every` rows (para.in) and, when max_rows > 0, after max_rows
+ * rows, where the call stops with *finished = 0. A completed run removes the
+ * checkpoint and sets *finished = 1. A resumed run truncates rows written after its
+ * checkpoint and writes the same bytes as an uninterrupted run. With max_rows <= 0
+ * and no checkpoint_every this is gqt_lsqt. para.in `output_moments` also appends
+ * each row's raw moments to <name>_moments.bin (16-byte header "GQTMOMv1",
+ * int32 number_of_moments, int32 0; then per row number_of_moments (re, im) doubles,
+ * little-endian). */
+gqt_status gqt_lsqt_run(const char* input_dir, int precision, int verbose, long long max_rows,
+                        int* finished);
 
 /* ---------------------------------------------------------------- no-allocation step */
 /* No counterpart in the reference. One fused Chebyshev step with its moment, the

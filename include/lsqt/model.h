@@ -62,6 +62,15 @@ public:
   long phase_seed = -1;
   bool verbose = true;
 
+  // Extensions (para.in keywords; the reference has neither): `output_moments`
+  // appends each row's raw moments to <name>_moments.bin; `checkpoint_every K`
+  // writes lsqt.checkpoint every K rows so that an interrupted run resumes.
+  bool output_moments = false;
+  int checkpoint_every = 0;
+  // The generator's state (with the one-time phase reseed flag), as text.
+  std::string rng_state() const;
+  void set_rng_state(const std::string& state);
+
   // Builds without printing or exiting: failures raise gqt_host::InputError.
   struct Quiet {};
   Model(std::string input_dir, Quiet);
