@@ -782,8 +782,19 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
 // access is a wide load. Same arithmetic per element as k_step; with FastArith the
 // moment uses the FP64 value of T_m before its FP32 rounding and plain FP64 per-thread
 // sums (a few dozen terms each), merged with TwoSum across lanes, blocks and the grid.
+// Register budgets of the batched steps, as blocks per SM, measured on B200 against the
+// compiler's own choice: k_step_vec at 4 (64 registers: +9 % for 16 FP32 vectors on
+// graphene, +7 % on cubic, +17 % for 32 vectors on the ELL arrays); k_step_multi at 3
+// with the coded table, 4 on the ELL arrays.
+constexpr int kVecMinBlocks = 4;
+template <bool C>
+constexpr int multi_min_blocks()
+{
+  return C ? 3 : 4;
+}
+
 template <typename VT2, int V, int W, int Z, class A, int MODE, bool DOT, bool C>
-__global__ void __launch_bounds__(kBlock) k_step_vec(Op op, const VT2* t0,
+__global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const VT2* t0,
                                                      const VT2* __restrict__ t1, VT2* out,
                                                      const VT2* __restrict__ left, Dot dot)
 {
@@ -947,7 +958,7 @@ __device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSu
 // of that realisation; slots of realisations it never meets are zeroed.
 // k_tile_reduce then sums the blocks per realisation in fixed order.
 template <typename VT2, int V, int W, int Z, class A, int MODE, bool C>
-__global__ void __launch_bounds__(kBlock) k_step_multi(Op op, const VT2* t0,
+__global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
                                                        const VT2* __restrict__ left, MultiDot md)
 {
