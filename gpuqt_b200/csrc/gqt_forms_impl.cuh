@@ -47,6 +47,27 @@ gqt_status launch_op(K* kernel, size_t total, const Op& op, Args... args)
   return GQT_OK;
 }
 
+// launch_op with programmatic stream serialisation: the kernel may start while the
+// previous kernel in the stream finishes, and must call pdl_wait before it reads or
+// writes anything a previous kernel produces (k_step does).
+template <typename... KArgs, typename... Args>
+gqt_status launch_op_pdl(void (*kernel)(Op, KArgs...), size_t total, const Op& op, Args... args)
+{
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid_for((const void*)kernel, total));
+  cfg.blockDim = dim3(kBlock);
+  cfg.dynamicSmemBytes = op_smem_bytes(op);
+  cfg.stream = stream();
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  GQT_CUDA(cudaLaunchKernelEx(&cfg, kernel, op, args...));
+  count_launches(1);
+  return GQT_OK;
+}
+
 template <typename K, typename... Args>
 gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
 {
@@ -105,14 +126,22 @@ struct OpImpl {
         }
         return run(std::integral_constant<int, W>{});
       }
+      // Programmatic dependent launch for the FP64 step (+1-2 % there; the FP32 step
+      // lost 7 % with it on B200).
+      auto go = [&](auto* kernel) -> gqt_status {
+        if constexpr (std::is_same<VT2, double2>::value)
+          return launch_op_pdl(kernel, total, op, a0, a1, o, l, d);
+        else
+          return launch_op(kernel, total, op, a0, a1, o, l, d);
+      };
       if (mode == kApply) {
         if (dot)
-          return launch_op(k_step<VT2, V, Z, A, kApply, true, C>, total, op, a0, a1, o, l, d);
-        return launch_op(k_step<VT2, V, Z, A, kApply, false, C>, total, op, a0, a1, o, l, d);
+          return go(k_step<VT2, V, Z, A, kApply, true, C>);
+        return go(k_step<VT2, V, Z, A, kApply, false, C>);
       }
       if (dot)
-        return launch_op(k_step<VT2, V, Z, A, kCheb, true, C>, total, op, a0, a1, o, l, d);
-      return launch_op(k_step<VT2, V, Z, A, kCheb, false, C>, total, op, a0, a1, o, l, d);
+        return go(k_step<VT2, V, Z, A, kCheb, true, C>);
+      return go(k_step<VT2, V, Z, A, kCheb, false, C>);
     });
   }
 

@@ -90,6 +90,19 @@ __device__ __forceinline__ Tables load_tables(const Op& op)
   return Tables{delta, hop, xx};
 }
 
+// Programmatic dependent launch: a step launched with the programmatic-serialisation
+// attribute may start while the previous kernel in its stream finishes. Before
+// pdl_wait it touches only what no kernel writes (the operator and its table); after
+// it, the previous grid has completed and its writes are visible. Each block calls
+// pdl_trigger once its main loop is done, so the next step's blocks can be scheduled
+// onto the SMs this grid frees while its last block combines the moment. Both are
+// no-ops in a launch without the attribute.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger()
+{
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Entry e = m * n + i of row i: neighbour j, hopping h, and the table row c (coded
 // form only) for ell_xx.
 template <bool C>
@@ -705,8 +718,10 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, co
       fetch_row<Z, C>(op, (int)(g / V), cur);
       if constexpr (kHops)
         fetch_hops<Z>(op, (int)(g / V), hc);
-      fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, sc);
     }
+    pdl_wait();
+    if (g < total)
+      fetch_streams<VT2, V, MODE, DOT>(op, g, t0, t1, left, sc);
     for (; g < total; g += stride) {
       const int i = (int)(g / V);
       const int v = (int)(g % V);
@@ -740,6 +755,7 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, co
       hc = hn;
     }
   } else {
+    pdl_wait();
     for (; g < total; g += stride) {
       const int i = (int)(g / V);
       const int v = (int)(g % V);
@@ -761,6 +777,7 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, co
         dot_term(re, im, stored(out, r), ld(left + g));
     }
   }
+  pdl_trigger();
   if constexpr (DOT)
     dot_finish<V>(re, im, dot);
 }
