@@ -460,6 +460,40 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / rate64
         out[k]["speedup_vs_fp64_ell"] = out[k]["site_moments_per_s"] / rate64_ell
     out["fp64_v1_site_moments_per_s"] = rate64
+
+    # Symmetric moment sets from half the Chebyshev steps (gqt_moments_doubled): the
+    # same moments (moments produced per second), equal to the direct ones up to
+    # rounding of the largest moment's order.
+    def doubled(X, V):
+        mu = torch.empty(2 * M * V, dtype=torch.float64, device="cuda")
+        g.moments_doubled_device(H, X, M, mu.data_ptr())
+        a, b = ev()
+        a.record(stream)
+        for _ in range(3):
+            g.moments_doubled_device(H, X, M, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        return V * n * M * 3 / (a.elapsed_time(b) / 1e3)
+
+    dr, di = g.moments_doubled(H, x64, M)
+    out["fp64_doubled"] = {
+        "site_moments_per_s": doubled(x64, 1),
+        "max_err_vs_direct": float(np.max(np.hypot(dr - r64, di - i64)) /
+                                   np.max(np.hypot(r64, i64))),
+        "speedup_vs_fp64": None}
+    out["fp64_doubled"]["speedup_vs_fp64"] = out["fp64_doubled"]["site_moments_per_s"] / rate64
+    vecs = [phi] + [m.initial_state() for _ in range(15)]
+    X16 = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
+                             nvec=16, precision=g.FP32)
+    r32, i32 = g.moments_doubled(H, X16, M)
+    out["fp32_v16_doubled"] = {
+        "site_moments_per_s": doubled(X16, 16),
+        "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32[0], i32[0]))}
+    out["fp32_v16_doubled"]["speedup_vs_fp64"] = (
+        out["fp32_v16_doubled"]["site_moments_per_s"] / rate64)
+    out["fp32_v16_doubled"]["speedup_vs_fp64_ell"] = (
+        out["fp32_v16_doubled"]["site_moments_per_s"] / rate64_ell)
+    del X16
     ach = fp64_bytes_per_site(coded=False) * rate64_ell / 1e9
     out["fp64_v1_ell"] = {"site_moments_per_s": rate64_ell, "achieved_gbs": ach,
                           "frac": ach / hbm_peak,

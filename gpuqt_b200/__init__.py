@@ -103,6 +103,8 @@ _SIGS = {
     "gqt_moments_form": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _dp]),
     "gqt_moments_device_form": (ctypes.c_int, [_vp, _vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "gqt_vec_convert": (ctypes.c_int, [_vp, _vp]),
+    "gqt_moments_doubled": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _dp, _dp]),
+    "gqt_moments_doubled_device": (ctypes.c_int, [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp]),
     "gqt_evolve": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp]),
     "gqt_evolvex": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_double, _vp]),
     "gqt_chebyshev_summation": (ctypes.c_int, [ctypes.c_int, _dp, _dp, ctypes.c_int, _dp,
@@ -483,6 +485,24 @@ def moments(H: Hamiltonian, left: Vector, right: Vector, n_moments: int,
     if right.nvec > 1:
         return re.reshape(right.nvec, n_moments), im.reshape(right.nvec, n_moments)
     return re, im
+
+
+def moments_doubled(H: Hamiltonian, state: Vector, n_moments: int, precision: int | None = None):
+    """mu_m = <state|T_m(H/E_max)|state> from n_moments / 2 Chebyshev steps
+    (gqt_moments_doubled); shapes as moments()."""
+    re = np.zeros(n_moments * state.nvec)
+    im = np.zeros(n_moments * state.nvec)
+    prec = state.precision if precision is None else precision
+    _call("gqt_moments_doubled", H.h, state.h, n_moments, prec, _dptr(re), _dptr(im))
+    if state.nvec > 1:
+        return re.reshape(state.nvec, n_moments), im.reshape(state.nvec, n_moments)
+    return re, im
+
+
+def moments_doubled_device(H: Hamiltonian, state: Vector, n_moments: int, mu_ptr: int,
+                           precision: int | None = None) -> None:
+    prec = state.precision if precision is None else precision
+    _call("gqt_moments_doubled_device", H.h, state.h, n_moments, prec, ctypes.c_void_p(mu_ptr))
 
 
 def autotune_nvec(H: Hamiltonian, precision: int, n_moments: int, candidates):

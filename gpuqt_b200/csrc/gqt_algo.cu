@@ -22,6 +22,7 @@ Workspace::~Workspace()
   cudaFree(dot.partials);
   cudaFree(dot.counter);
   cudaFree(mu);
+  cudaFree(pairs);
   if (ev_in)
     cudaEventDestroy(ev_in);
   if (ev_out)
@@ -216,6 +217,39 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
     prev = cur;
     cur = out;
   }
+  return GQT_OK;
+}
+
+// The symmetric moment set mu_m = <phi|T_m|phi>, m < M, from K = M / 2 steps: slot 0
+// of `pairs` gets mu_0, slot k the pair <T_k|T_k>, <T_{k-1}|T_k> of step k, and
+// k_pair_moments turns them into mu (layout [m][v]). The left stream of the direct
+// loop is not read, and the recurrence runs half as many steps.
+gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_vec* phi, int M,
+                                double2* mu, double2* pairs, void* A, void* B, DotScratch* ds)
+{
+  const Op op = make_op(h, phi->nvec);
+  const int V = phi->nvec;
+  const size_t total = (size_t)h->n * V;
+  Dot d{ds->partials, ds->counter, pairs};
+  GQT_TRY(f->dot(total, phi->data, phi->data, d));
+  const int K = M / 2;
+  if (K >= 1) {
+    d.mu = pairs + (size_t)2 * V;
+    GQT_TRY(f->step_pair(op, kApply, nullptr, phi->data, A, d));
+    const void* prev = phi->data;
+    void* cur = A;
+    for (int k = 2; k <= K; ++k) {
+      void* out = (prev == phi->data) ? B : (void*)prev;
+      d.mu = pairs + (size_t)k * 2 * V;
+      GQT_TRY(f->step_pair(op, kCheb, prev, cur, out, d));
+      prev = cur;
+      cur = out;
+    }
+  }
+  const int n = M * V;
+  k_pair_moments<double2><<<(n + kBlock - 1) / kBlock, kBlock, 0, stream()>>>(pairs, M, V, mu);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
   return GQT_OK;
 }
 
@@ -461,21 +495,45 @@ static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const g
   return GQT_OK;
 }
 
-extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
-                                         const gqt_vec* right, int M, void* mu_dev)
+// The moment loop (direct, or the symmetric pair loop) as one CUDA graph launch.
+static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                              int M, void* mu_dev, bool pair, const char* w)
 {
   const FormOps* f;
   void *A, *B;
   DotScratch* ds;
   GQT_TRY(moments_prepare(h, left, right, M, &f, &A, &B, &ds));
   if (!mu_dev)
-    return fail(GQT_ERR_ARG, "gqt_moments_device: null output");
+    return fail(GQT_ERR_ARG, "%s: null output", w);
   Workspace& ws = *h->ws;
   cudaStream_t s = stream();
+  if (pair) {
+    if (h->n_real > 1)
+      return fail(GQT_ERR_STATE, "%s: not available for a realisation batch", w);
+    if (!h->hermitian)
+      return fail(GQT_ERR_STATE,
+                  "%s: the operator is not Hermitian (the doubling identity needs H = H^+)", w);
+    if (right->nvec > 16)
+      return fail(GQT_ERR_ARG, "%s: at most 16 vectors (got %d)", w, right->nvec);
+    const size_t need = (size_t)(M / 2 + 1) * 2 * right->nvec * sizeof(double2);
+    if (ws.pairs_bytes < need) {
+      cudaStreamSynchronize(s);
+      cudaFree(ws.pairs);
+      ws.pairs = nullptr;
+      ws.pairs_bytes = 0;
+      GQT_CUDA(cudaMalloc(&ws.pairs, need));
+      ws.pairs_bytes = need;
+      // Graphs captured with the old buffer can never run again.
+      for (auto& kv : ws.graphs)
+        cudaGraphExecDestroy(kv.second);
+      ws.graphs.clear();
+    }
+  }
 
   // The n_moments launches are captured once per (left, right, M, output, form) and
   // replayed as one graph launch afterwards.
-  Workspace::GraphKey key{left->data, right->data, M, mu_dev, right->precision, right->nvec};
+  Workspace::GraphKey key{left->data, right->data,      M, mu_dev,
+                          right->precision, right->nvec, pair ? 1 : 0};
   auto it = ws.graphs.find(key);
   if (it == ws.graphs.end()) {
     if (!ws.capture_stream) {
@@ -490,7 +548,8 @@ extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
     gqt_status st = GQT_OK;
     if (e == cudaSuccess) {
       const uint64_t before = gqt_launch_count();
-      st = moment_launches(h, f, left, right, M, (double2*)mu_dev, A, B, ds);
+      st = pair ? moment_launches_pair(h, f, right, M, (double2*)mu_dev, ws.pairs, A, B, ds)
+                : moment_launches(h, f, left, right, M, (double2*)mu_dev, A, B, ds);
       // Captured launches run later, when the graph is launched.
       gqt_reset_launch_count();
       count_launches(before);
@@ -521,6 +580,12 @@ extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
   GQT_CUDA(cudaEventRecord(ws.ev_out, ws.capture_stream));
   GQT_CUDA(cudaStreamWaitEvent(s, ws.ev_out, 0));
   return GQT_OK;
+}
+
+extern "C" gqt_status gqt_moments_device(const gqt_ham* h, const gqt_vec* left,
+                                         const gqt_vec* right, int M, void* mu_dev)
+{
+  return moments_run(h, left, right, M, mu_dev, false, "gqt_moments_device");
 }
 
 static gqt_status convert_data(int n, int nvec, int from, const void* src, int to, void* dst)
@@ -554,15 +619,15 @@ extern "C" gqt_status gqt_vec_convert(gqt_vec* dst, const gqt_vec* src)
   return convert_data(src->n, src->nvec, src->precision, src->data, dst->precision, dst->data);
 }
 
-extern "C" gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
-                                              const gqt_vec* right, int M, int precision,
-                                              void* mu_dev)
+// moments_run in another arithmetic form than the vectors' (converted copies).
+static gqt_status moments_form_run(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                                   int M, int precision, void* mu_dev, bool pair,
+                                   const char* w)
 {
-  const char* w = "gqt_moments_device_form";
   if (!h || !left || !right || !left->data || !right->data)
     return fail(GQT_ERR_ARG, "%s: null argument", w);
   if (precision == right->precision && precision == left->precision)
-    return gqt_moments_device(h, left, right, M, mu_dev);
+    return moments_run(h, left, right, M, mu_dev, pair, w);
   if (!form_ops(precision, right->nvec))
     return fail(GQT_ERR_ARG, "%s: form %d has no %d-vector launch", w, precision, right->nvec);
   if (left->n != right->n || left->nvec != right->nvec)
@@ -584,7 +649,22 @@ extern "C" gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* l
   R.bytes = L.bytes = bytes;
   R.data = rc;
   L.data = same ? rc : lc;
-  return gqt_moments_device(h, &L, &R, M, mu_dev);
+  return moments_run(h, &L, &R, M, mu_dev, pair, w);
+}
+
+extern "C" gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
+                                              const gqt_vec* right, int M, int precision,
+                                              void* mu_dev)
+{
+  return moments_form_run(h, left, right, M, precision, mu_dev, false,
+                          "gqt_moments_device_form");
+}
+
+extern "C" gqt_status gqt_moments_doubled_device(const gqt_ham* h, const gqt_vec* state, int M,
+                                                 int precision, void* mu_dev)
+{
+  return moments_form_run(h, state, state, M, precision, mu_dev, true,
+                          "gqt_moments_doubled_device");
 }
 
 extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
@@ -595,18 +675,19 @@ extern "C" gqt_status gqt_moments(const gqt_ham* h, const gqt_vec* left, const g
   return gqt_moments_form(h, left, right, M, right->precision, mu_re, mu_im);
 }
 
-extern "C" gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left,
-                                       const gqt_vec* right, int M, int precision,
-                                       double* mu_re, double* mu_im)
+// A moment loop into the workspace's device buffer, then to host arrays [vector][m].
+static gqt_status moments_host(const gqt_ham* h, const gqt_vec* left, const gqt_vec* right,
+                               int M, int precision, bool pair, double* mu_re, double* mu_im,
+                               const char* w)
 {
   if (!mu_re || !mu_im)
-    return fail(GQT_ERR_ARG, "gqt_moments: null output");
+    return fail(GQT_ERR_ARG, "%s: null output", w);
   if (!h)
-    return fail(GQT_ERR_ARG, "gqt_moments: null Hamiltonian");
+    return fail(GQT_ERR_ARG, "%s: null Hamiltonian", w);
   if (!right)
-    return fail(GQT_ERR_ARG, "gqt_moments: null vector");
+    return fail(GQT_ERR_ARG, "%s: null vector", w);
   if (M < 1)
-    return fail(GQT_ERR_ARG, "gqt_moments: number of moments must be > 0 (got %d)", M);
+    return fail(GQT_ERR_ARG, "%s: number of moments must be > 0 (got %d)", w, M);
   Workspace& ws = *h->ws;
   const int V = right->nvec * h->n_real;  // results per moment: [r][vector]
   const size_t need = (size_t)M * V * sizeof(double2);
@@ -622,7 +703,7 @@ extern "C" gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left,
       cudaGraphExecDestroy(kv.second);
     ws.graphs.clear();
   }
-  GQT_TRY(gqt_moments_device_form(h, left, right, M, precision, ws.mu));
+  GQT_TRY(moments_form_run(h, left, right, M, precision, ws.mu, pair, w));
   std::vector<double2> host((size_t)M * V);
   GQT_CUDA(cudaMemcpyAsync(host.data(), ws.mu, need, cudaMemcpyDeviceToHost, stream()));
   GQT_CUDA(cudaStreamSynchronize(stream()));
@@ -632,6 +713,19 @@ extern "C" gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left,
       mu_im[(size_t)k * M + m] = host[(size_t)m * V + k].y;
     }
   return GQT_OK;
+}
+
+extern "C" gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left,
+                                       const gqt_vec* right, int M, int precision,
+                                       double* mu_re, double* mu_im)
+{
+  return moments_host(h, left, right, M, precision, false, mu_re, mu_im, "gqt_moments");
+}
+
+extern "C" gqt_status gqt_moments_doubled(const gqt_ham* h, const gqt_vec* state, int M,
+                                          int precision, double* mu_re, double* mu_im)
+{
+  return moments_host(h, state, state, M, precision, true, mu_re, mu_im, "gqt_moments_doubled");
 }
 
 // ------------------------------------------------------------------ time evolution

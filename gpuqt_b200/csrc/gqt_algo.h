@@ -24,8 +24,11 @@ struct Workspace {
   size_t mu_bytes = 0;
   cudaStream_t capture_stream = nullptr;  // used when the caller's stream is the legacy one
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
-  // Instantiated moment loops: (left, right, n_moments, mu, precision, nvec).
-  using GraphKey = std::tuple<const void*, const void*, int, void*, int, int>;
+  double2* pairs = nullptr;  // pair products of the symmetric moment loop
+  size_t pairs_bytes = 0;
+  // Instantiated moment loops: (left, right, n_moments, mu, precision, nvec, loop),
+  // loop 0 the direct one, 1 the symmetric (pair) one.
+  using GraphKey = std::tuple<const void*, const void*, int, void*, int, int, int>;
   std::map<GraphKey, cudaGraphExec_t> graphs;
   ~Workspace();
 };

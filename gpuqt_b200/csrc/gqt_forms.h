@@ -15,6 +15,10 @@ struct OpFns {
   // out = H t1 (mode kApply) or 2 H t1 - t0 (kCheb); dot != nullptr fuses <left|out>.
   gqt_status (*step)(const Op& op, int mode, const void* t0, const void* t1, void* out,
                      const void* left, const Dot* dot);
+  // The same step fusing the pair <T_k|T_k>, <T_{k-1}|T_k> (t1 = T_{k-1}) of a symmetric
+  // moment set into dot->mu[0 .. 2 nvec); GQT_ERR_ARG for more than 16 vectors.
+  gqt_status (*step_pair)(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                          const Dot& dot);
   // One step of a realisation batch (mode kDotOnly, kApply or kCheb) with moments per
   // realisation.
   gqt_status (*step_multi)(const Op& op, int mode, const void* t0, const void* t1, void* out,
@@ -49,6 +53,11 @@ struct FormOps {
                   const void* left, const Dot* d) const
   {
     return of(op).step(op, mode, t0, t1, out, left, d);
+  }
+  gqt_status step_pair(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                       const Dot& d) const
+  {
+    return of(op).step_pair(op, mode, t0, t1, out, d);
   }
   gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1, void* out,
                         const void* left, const MultiDot& md) const

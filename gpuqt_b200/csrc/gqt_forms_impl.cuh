@@ -145,6 +145,36 @@ struct OpImpl {
     });
   }
 
+  static gqt_status step_pair(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                              const Dot& d)
+  {
+    if constexpr (V > 16) {
+      return fail(GQT_ERR_ARG, "symmetric moments: at most 16 vectors per launch (got %d)", V);
+    } else {
+      const VT2* a0 = (const VT2*)t0;
+      const VT2* a1 = (const VT2*)t1;
+      VT2* o = (VT2*)out;
+      return with_z(op.z, [&](auto zc) -> gqt_status {
+        constexpr int Z = decltype(zc)::value;
+        if constexpr (W > 1) {
+          const size_t items = (size_t)op.n * (V / W);
+          if (mode == kApply)
+            return launch_op(k_step_vec<VT2, V, W, Z, A, kApply, kDotPair, C>, items, op, a0, a1,
+                             o, (const VT2*)nullptr, d);
+          return launch_op(k_step_vec<VT2, V, W, Z, A, kCheb, kDotPair, C>, items, op, a0, a1, o,
+                           (const VT2*)nullptr, d);
+        } else {
+          const size_t total = (size_t)op.n * V;
+          if (mode == kApply)
+            return launch_op(k_step<VT2, V, Z, A, kApply, kDotPair, C>, total, op, a0, a1, o,
+                             (const VT2*)nullptr, d);
+          return launch_op(k_step<VT2, V, Z, A, kCheb, kDotPair, C>, total, op, a0, a1, o,
+                           (const VT2*)nullptr, d);
+        }
+      });
+    }
+  }
+
   static gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1,
                                void* out, const void* left, const MultiDot& md_in)
   {
@@ -218,7 +248,7 @@ struct OpImpl {
     });
   }
 
-  static OpFns fns() { return OpFns{step, step_multi, xop, cheb2, cheb2x}; }
+  static OpFns fns() { return OpFns{step, step_pair, step_multi, xop, cheb2, cheb2x}; }
 };
 
 template <typename VT2, int V, class A>

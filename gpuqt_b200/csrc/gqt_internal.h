@@ -82,6 +82,7 @@ struct gqt_ham {
   double2* code_hop = nullptr;  // [n_codes]
   double* code_xx = nullptr;    // [n_codes]
   int n_codes = 0;
+  int hermitian = 0;  // H = H^+ (checked at upload; the symmetric moment loop needs it)
   int use_codes = 0;            // kernels read the codes (default when they exist)
   // Realisation batch (gqt_ham_create_batch): n_real > 1 block-diagonal models, each
   // padded to whole tiles and pre-divided by its own E_max (energy_max is then 1).

@@ -462,6 +462,12 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
 
 enum StepMode { kApply = 0, kCheb = 1 };
 
+// What a step fuses after writing T_k (the DOT template parameter): nothing; the moment
+// <left|T_k>; or the pair <T_k|T_k>, <T_{k-1}|T_k> of a symmetric moment set (left =
+// right = phi), from which T_j T_k = (T_{j+k} + T_{|j-k|}) / 2 gives mu_2k and
+// mu_{2k-1} (k_pair_moments).
+enum DotMode { kNoDot = 0, kDotLeft = 1, kDotPair = 2 };
+
 // Grid-stride loop shape of each operator kernel, per format (C), storage type and
 // row bound Z. The pipelined loop loads the next element's row (and, in k_step, its
 // streamed inputs) one iteration ahead, so an iteration waits on one memory round
@@ -665,7 +671,7 @@ struct Streams {
   double2 x, y0, l;
 };
 
-template <typename VT2, int V, int MODE, bool DOT>
+template <typename VT2, int V, int MODE, int DOT>
 __device__ __forceinline__ void fetch_streams(const Op& op, size_t g, const VT2* t0,
                                               const VT2* __restrict__ t1,
                                               const VT2* __restrict__ left, Streams& s)
@@ -676,8 +682,21 @@ __device__ __forceinline__ void fetch_streams(const Op& op, size_t g, const VT2*
   s.l = s.y0;
   if constexpr (MODE == kCheb)
     s.y0 = ld(t0 + g);
-  if constexpr (DOT)
+  if constexpr (DOT == kDotLeft)
     s.l = ld(left + g);
+}
+
+// The fused moment terms of one element: o = T_k as stored, x = T_{k-1}, l = left.
+template <int DOT>
+__device__ __forceinline__ void step_dot(CSum (&re)[2], CSum (&im)[2], double2 o, double2 x,
+                                         double2 l)
+{
+  if constexpr (DOT == kDotLeft) {
+    dot_term(re[0], im[0], o, l);
+  } else if constexpr (DOT == kDotPair) {
+    dot_term(re[0], im[0], o, o);
+    dot_term(re[1], im[1], o, x);
+  }
 }
 
 // out = H t1 / E_max (kApply) or out = 2 H t1 / E_max - t0 (kCheb), optionally fused
@@ -699,15 +718,16 @@ constexpr int step_min_blocks()
   return Z >= 6 ? 2 : 3;
 }
 
-template <typename VT2, int V, int Z, class A, int MODE, bool DOT, bool C>
+template <typename VT2, int V, int Z, class A, int MODE, int DOT, bool C>
 __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, const VT2* t0,
                                                  const VT2* __restrict__ t1, VT2* out,
                                                  const VT2* __restrict__ left, Dot dot)
 {
+  static_assert(DOT != kDotPair || V == 1, "pair moments: one vector per thread");
   const Tables tb = load_tables<C>(op);
   const size_t total = (size_t)op.n * V;
   const size_t stride = (size_t)gridDim.x * kBlock;
-  CSum re{0.0, 0.0}, im{0.0, 0.0};
+  CSum re[2] = {{0.0, 0.0}, {0.0, 0.0}}, im[2] = {{0.0, 0.0}, {0.0, 0.0}};
   size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
   if constexpr (Z > 0 && pipelined<kPipeStep, C, VT2, Z>()) {
     RowIdx<Z> cur;
@@ -749,8 +769,7 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, co
       }
       const double2 r = make_double2(tr, ti);
       st(out + g, r);
-      if constexpr (DOT)
-        dot_term(re, im, stored(out, r), s.l);
+      step_dot<DOT>(re, im, stored(out, r), s.x, s.l);
       cur = nxt;
       hc = hn;
     }
@@ -773,13 +792,17 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, co
       }
       const double2 r = make_double2(tr, ti);
       st(out + g, r);
-      if constexpr (DOT)
-        dot_term(re, im, stored(out, r), ld(left + g));
+      if constexpr (DOT == kDotLeft)
+        step_dot<DOT>(re, im, stored(out, r), x, ld(left + g));
+      else
+        step_dot<DOT>(re, im, stored(out, r), x, x);
     }
   }
   pdl_trigger();
-  if constexpr (DOT)
-    dot_finish<V>(re, im, dot);
+  if constexpr (DOT == kDotLeft)
+    dot_finish<V>(re[0], im[0], dot);
+  else if constexpr (DOT == kDotPair)
+    dot_finish_w<2, 2>(re, im, dot);
 }
 
 // <left|state> alone (moment 0).
@@ -810,7 +833,7 @@ constexpr int multi_min_blocks()
   return C ? 3 : 4;
 }
 
-template <typename VT2, int V, int W, int Z, class A, int MODE, bool DOT, bool C>
+template <typename VT2, int V, int W, int Z, class A, int MODE, int DOT, bool C>
 __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const VT2* t0,
                                                      const VT2* __restrict__ t1, VT2* out,
                                                      const VT2* __restrict__ left, Dot dot)
@@ -819,9 +842,11 @@ __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const
   constexpr int kTps = V / W;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
   const size_t items = (size_t)op.n * kTps;
-  CSum re[W], im[W];
+  // Pair moments keep two sums per vector: [2w] <T_k|T_k>, [2w + 1] <T_{k-1}|T_k>.
+  constexpr int kSums = DOT == kDotPair ? 2 * W : W;
+  CSum re[kSums], im[kSums];
 #pragma unroll
-  for (int k = 0; k < W; ++k)
+  for (int k = 0; k < kSums; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
   // Pipelined as in k_step where the policy says so: the next item's row first.
   constexpr bool kPre = Z > 0 && pipelined<kPipeStepVec, C, VT2, Z>();
@@ -891,7 +916,7 @@ __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const
         r[k] = make_double2(A::scale(tr[k], op), A::scale(ti[k], op));
     }
     stw<W>(out + base, r);
-    if constexpr (DOT) {
+    if constexpr (DOT == kDotLeft) {
       double2 l[W];
       ldw<W>(left + base, l);
 #pragma unroll
@@ -903,12 +928,28 @@ __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const
           im[k].s = fma(r[k].y, l[k].x, fma(-r[k].x, l[k].y, im[k].s));
         }
       }
+    } else if constexpr (DOT == kDotPair) {
+      // x holds T_{k-1} as stored; T_k as stored is stored(out, r).
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const double2 o = stored(out, r[k]);
+        if constexpr (kExact) {
+          dot_term(re[2 * k], im[2 * k], o, o);
+          dot_term(re[2 * k + 1], im[2 * k + 1], o, x[k]);
+        } else {
+          re[2 * k].s = fma(o.x, o.x, fma(o.y, o.y, re[2 * k].s));
+          re[2 * k + 1].s = fma(o.x, x[k].x, fma(o.y, x[k].y, re[2 * k + 1].s));
+          im[2 * k + 1].s = fma(o.y, x[k].x, fma(-o.x, x[k].y, im[2 * k + 1].s));
+        }
+      }
     }
     if constexpr (kPre)
       cur = nxt;
   }
-  if constexpr (DOT)
+  if constexpr (DOT == kDotLeft)
     dot_finish_w<V, W>(re, im, dot);
+  else if constexpr (DOT == kDotPair)
+    dot_finish_w<2 * V, 2 * W>(re, im, dot);
 }
 
 // ------------------------------------------------------------------ realisation batches
@@ -1464,6 +1505,36 @@ __global__ void __launch_bounds__(kBlock) k_segment_sum(const double2* __restric
     }
     out[blockIdx.x] = make_double2(__dadd_rn(r.s, r.c), __dadd_rn(i.s, i.c));
   }
+}
+
+// Moments of a symmetric set from its pair products: slot k (1 <= k <= K) of `pairs`
+// holds, per vector v, A_k = <T_k|T_k> at [k][2v] and B_k = <T_{k-1}|T_k> at
+// [k][2v + 1]; slot 0 holds mu_0 = <phi|phi> at [0][v]. With T_j T_k = (T_{j+k} +
+// T_{|j-k|}) / 2: mu_1 = B_1, mu_2k = 2 A_k - mu_0, mu_{2k-1} = 2 B_k - mu_1.
+// Writes mu[m][v] for m < M (the layout of the direct moment loop).
+template <typename T2>
+__global__ void __launch_bounds__(kBlock) k_pair_moments(const T2* __restrict__ pairs, int M,
+                                                         int V, T2* __restrict__ mu)
+{
+  const int t = blockIdx.x * kBlock + threadIdx.x;
+  if (t >= M * V)
+    return;
+  const int m = t / V, v = t % V;
+  const T2 mu0 = pairs[v];
+  T2 r;
+  if (m == 0) {
+    r = mu0;
+  } else if (m == 1) {
+    r = pairs[(size_t)2 * V + 2 * v + 1];
+  } else if ((m & 1) == 0) {
+    const T2 a = pairs[(size_t)(m / 2) * 2 * V + 2 * v];
+    r = make_double2(__dsub_rn(__dmul_rn(2.0, a.x), mu0.x), __dsub_rn(__dmul_rn(2.0, a.y), mu0.y));
+  } else {
+    const T2 mu1 = pairs[(size_t)2 * V + 2 * v + 1];
+    const T2 b = pairs[(size_t)((m + 1) / 2) * 2 * V + 2 * v + 1];
+    r = make_double2(__dsub_rn(__dmul_rn(2.0, b.x), mu1.x), __dsub_rn(__dmul_rn(2.0, b.y), mu1.y));
+  }
+  mu[t] = r;
 }
 
 // dst = src across storage forms (FP64 <-> FP32).

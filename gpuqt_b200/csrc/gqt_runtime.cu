@@ -2,6 +2,7 @@
 // Hamiltonian handles. See include/gpuqt.h for the contract of each entry point.
 #include <cstdarg>
 #include <cstdio>
+#include <cmath>
 #include <cstring>
 #include <mutex>
 #include <unordered_map>
@@ -464,6 +465,48 @@ bool build_codes(const Packed& P, std::vector<uint8_t>& codes, std::vector<int>&
   return true;
 }
 
+// H = H^+ for the packed operator: for every pair of sites, the hoppings of the
+// entries i -> j summed equal the conjugate of those of j -> i (relative 1e-12).
+// Rows are short (z entries), so this is O(n z^2).
+bool is_hermitian(const Packed& P)
+{
+  auto row_len = [&](int i) { return P.uniform ? P.z : P.nn[i]; };
+  auto entry = [&](int i, int m) { return (size_t)m * P.n + i; };
+  for (int i = 0; i < P.n; ++i) {
+    const int ci = row_len(i);
+    for (int m = 0; m < ci; ++m) {
+      const int j = P.nl[entry(i, m)];
+      bool first = true;  // each distinct neighbour once
+      for (int q = 0; q < m; ++q)
+        if (P.nl[entry(i, q)] == j)
+          first = false;
+      if (!first)
+        continue;
+      double sr = 0, si = 0, tr = 0, ti = 0, mag = 0;
+      for (int q = m; q < ci; ++q)
+        if (P.nl[entry(i, q)] == j) {
+          sr += P.hop[entry(i, q)].x;
+          si += P.hop[entry(i, q)].y;
+          mag += std::fabs(P.hop[entry(i, q)].x) + std::fabs(P.hop[entry(i, q)].y);
+        }
+      const int cj = row_len(j);
+      for (int q = 0; q < cj; ++q)
+        if (P.nl[entry(j, q)] == i) {
+          tr += P.hop[entry(j, q)].x;
+          ti += P.hop[entry(j, q)].y;
+        }
+      if (j == i) {  // an entry to the site itself must be real
+        if (std::fabs(si) > 1e-12 * mag)
+          return false;
+        continue;
+      }
+      if (std::fabs(sr - tr) > 1e-12 * mag || std::fabs(si + ti) > 1e-12 * mag)
+        return false;
+    }
+  }
+  return true;
+}
+
 gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
 {
   const size_t pairs = (size_t)P.n * P.z;
@@ -503,6 +546,7 @@ gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ha
     h->n_codes = (int)nc;
     h->use_codes = 1;
   }
+  h->hermitian = is_hermitian(P) ? 1 : 0;
   h->ws.reset(new_workspace());
   return GQT_OK;
 }

@@ -94,7 +94,8 @@ uint64_t run_fingerprint(const Model& model, int precision)
   w.put<int32_t>(model.number_of_local_orbitals);
   const int flags = (model.calculate_vac0 ? 1 : 0) | (model.calculate_vac ? 2 : 0) |
                     (model.calculate_msd ? 4 : 0) | (model.calculate_spin ? 8 : 0) |
-                    (model.calculate_ldos ? 16 : 0) | (model.output_moments ? 32 : 0);
+                    (model.calculate_ldos ? 16 : 0) | (model.output_moments ? 32 : 0) |
+                    (model.kpm_doubling ? 64 : 0);
   w.put<int32_t>(flags);
   w.put<int32_t>(precision);
   w.put<double>(model.energy_max);

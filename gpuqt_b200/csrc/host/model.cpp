@@ -149,6 +149,8 @@ void Model::initialize_parameters()
       ss >> phase_seed;
     } else if (token == "output_moments") {
       output_moments = true;
+    } else if (token == "kpm_doubling") {
+      kpm_doubling = true;
     } else if (token == "checkpoint_every") {
       ss >> checkpoint_every;
       if (!ss || checkpoint_every < 1)
@@ -158,7 +160,7 @@ void Model::initialize_parameters()
           "\nValid keywords include: model anderson_disorder charged_impurity "
           "vacancy_disorder calculate_vac0 calculate_vac calculate_msd calculate_spin "
           "calculate_ldos number_of_random_vectors number_of_moments energy_max seed "
-          "disorder_seed phase_seed output_moments checkpoint_every");
+          "disorder_seed phase_seed output_moments checkpoint_every kpm_doubling");
     }
   }
   verify_parameters();

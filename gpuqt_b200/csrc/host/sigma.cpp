@@ -23,6 +23,13 @@ void find_moments_chebyshev(Model& model, Hamiltonian& H, Vector& state_left,
   // One fused step+moment kernel per moment, replayed as a CUDA graph, in the form
   // Vector::moment_precision; the moments land in `output` (FP64, number_of_moments
   // entries) on the device.
+  if (model.kpm_doubling && &state_left == &state_right) {
+    // A symmetric set from half the steps (para.in kpm_doubling).
+    check(gqt_moments_doubled_device(H.handle(), state_right.handle(), model.number_of_moments,
+                                     Vector::moment_precision, gqt_vec_data(output.handle())),
+          "find_moments_chebyshev");
+    return;
+  }
   check(gqt_moments_device_form(H.handle(), state_left.handle(), state_right.handle(),
                                 model.number_of_moments, Vector::moment_precision,
                                 gqt_vec_data(output.handle())),

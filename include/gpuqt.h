@@ -216,6 +216,18 @@ gqt_status gqt_moments_form(const gqt_ham* h, const gqt_vec* left, const gqt_vec
 gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
                                    const gqt_vec* right, int n_moments, int precision,
                                    void* mu_dev);
+/* The symmetric moment set mu_m = <phi|T_m(H~)|phi>, m < n_moments, from n_moments / 2
+ * Chebyshev steps, by T_j T_k = (T_{j+k} + T_{|j-k|}) / 2 (KPM "doubling": each step
+ * fuses <T_k|T_k> and <T_{k-1}|T_k>; mu_2k = 2 <T_k|T_k> - mu_0, mu_{2k-1} =
+ * 2 <T_{k-1}|T_k> - mu_1). No counterpart in the reference, whose loop takes n_moments
+ * steps (find_moments_chebyshev, src/sigma.cu:33-61, with left = right): same moments
+ * up to rounding of order 1e-15 mu_0 per moment in the FP64 form, not bit for bit.
+ * precision as in gqt_moments_form; at most 16 vectors; not for realisation batches.
+ * Outputs as gqt_moments (host) / gqt_moments_device (device, [m][vector] double2). */
+gqt_status gqt_moments_doubled(const gqt_ham* h, const gqt_vec* state, int n_moments,
+                               int precision, double* mu_re, double* mu_im);
+gqt_status gqt_moments_doubled_device(const gqt_ham* h, const gqt_vec* state, int n_moments,
+                                      int precision, void* mu_dev);
 /* dst = src across forms (FP64 <-> FP32, same sites and vector count); rounds to
  * nearest when narrowing. */
 gqt_status gqt_vec_convert(gqt_vec* dst, const gqt_vec* src);

@@ -62,11 +62,14 @@ public:
   long phase_seed = -1;
   bool verbose = true;
 
-  // Extensions (para.in keywords; the reference has neither): `output_moments`
+  // Extensions (para.in keywords; the reference has none of them): `output_moments`
   // appends each row's raw moments to <name>_moments.bin; `checkpoint_every K`
   // writes lsqt.checkpoint every K rows so that an interrupted run resumes.
   bool output_moments = false;
   int checkpoint_every = 0;
+  // `kpm_doubling`: symmetric moment sets (DOS, VAC0, MSD, LDOS) from half the
+  // Chebyshev steps (gqt_moments_doubled); equal to the direct moments up to rounding.
+  bool kpm_doubling = false;
   // The generator's state (with the one-time phase reseed flag), as text.
   std::string rng_state() const;
   void set_rng_state(const std::string& state);
