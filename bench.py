@@ -568,7 +568,25 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
     x0 = g.Vector.from_host(per0[0][0][0], per0[0][1][0])
     r64, i64 = g.moments(H0, x0, x0, moments)
     err = dos_error(g, m0, (r64, i64), (r32[0, 0], i32[0, 0]))
+    # The same batch as symmetric moment sets from half the steps (gqt_moments_doubled).
+    g.moments_doubled_device(B, X, moments, mu.data_ptr())
+    torch.cuda.synchronize()
+    dbl_ms = 0.0
+    for k in range(blocks):
+        if k:
+            fill()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.moments_doubled_device(B, X, moments, mu.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        dbl_ms += a.elapsed_time(b)
+    X.upload(*B.scatter(per0))
+    q32, j32 = g.moments_doubled(B, X, moments)
+    dbl_err = dos_error(g, m0, (r64, i64), (q32[0, 0], j32[0, 0]))
     return {"realisations": [[m.n, round(m.energy_max, 4)] for m in models],
+            "doubled": {"site_moments_per_s": vectors * sites * moments / (dbl_ms / 1e3),
+                        "ms_total": dbl_ms, "dos_err_vs_fp64": dbl_err},
             "sites": sites, "padded_sites": B.n, "vectors": vectors, "moments": moments,
             "operator_format": "coded" if B.format == g.FORMAT_CODED else "ell",
             "autotuned_vectors_per_launch": V, "autotune_rates": rates,

@@ -490,10 +490,13 @@ def moments(H: Hamiltonian, left: Vector, right: Vector, n_moments: int,
 def moments_doubled(H: Hamiltonian, state: Vector, n_moments: int, precision: int | None = None):
     """mu_m = <state|T_m(H/E_max)|state> from n_moments / 2 Chebyshev steps
     (gqt_moments_doubled); shapes as moments()."""
-    re = np.zeros(n_moments * state.nvec)
-    im = np.zeros(n_moments * state.nvec)
+    R = getattr(H, "n_real", 1)
+    re = np.zeros(n_moments * state.nvec * R)
+    im = np.zeros(n_moments * state.nvec * R)
     prec = state.precision if precision is None else precision
     _call("gqt_moments_doubled", H.h, state.h, n_moments, prec, _dptr(re), _dptr(im))
+    if R > 1:
+        return re.reshape(R, state.nvec, n_moments), im.reshape(R, state.nvec, n_moments)
     if state.nvec > 1:
         return re.reshape(state.nvec, n_moments), im.reshape(state.nvec, n_moments)
     return re, im

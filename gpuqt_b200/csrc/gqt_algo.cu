@@ -230,6 +230,32 @@ gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_ve
   const Op op = make_op(h, phi->nvec);
   const int V = phi->nvec;
   const size_t total = (size_t)h->n * V;
+  if (h->n_real > 1) {
+    // Realisation batch: slot 0 holds mu_0 per (realisation, vector), slot k the pairs
+    // [r][2v + t]; k_pair_moments then runs over R * V flattened moments.
+    const int RV = h->n_real * V;
+    MultiDot md{ds->partials, pairs, h->tile_first, h->n_tiles, h->tile_sites, h->n_real, 0};
+    GQT_TRY(f->step_multi(op, kDotOnly, nullptr, phi->data, nullptr, phi->data, md));
+    const int K = M / 2;
+    if (K >= 1) {
+      md.mu = pairs + (size_t)2 * RV;
+      GQT_TRY(f->step_multi(op, kApply, nullptr, phi->data, A, nullptr, md, kDotPair));
+      const void* prev = phi->data;
+      void* cur = A;
+      for (int k = 2; k <= K; ++k) {
+        void* out = (prev == phi->data) ? B : (void*)prev;
+        md.mu = pairs + (size_t)k * 2 * RV;
+        GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, nullptr, md, kDotPair));
+        prev = cur;
+        cur = out;
+      }
+    }
+    const int n = M * RV;
+    k_pair_moments<double2><<<(n + kBlock - 1) / kBlock, kBlock, 0, stream()>>>(pairs, M, RV, mu);
+    count_launches(1);
+    GQT_CUDA(cudaGetLastError());
+    return GQT_OK;
+  }
   Dot d{ds->partials, ds->counter, pairs};
   GQT_TRY(f->dot(total, phi->data, phi->data, d));
   const int K = M / 2;
@@ -508,14 +534,14 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
   Workspace& ws = *h->ws;
   cudaStream_t s = stream();
   if (pair) {
-    if (h->n_real > 1)
-      return fail(GQT_ERR_STATE, "%s: not available for a realisation batch", w);
     if (!h->hermitian)
       return fail(GQT_ERR_STATE,
                   "%s: the operator is not Hermitian (the doubling identity needs H = H^+)", w);
-    if (right->nvec > 16)
+    if (h->n_real == 1 && right->nvec > 16)
       return fail(GQT_ERR_ARG, "%s: at most 16 vectors (got %d)", w, right->nvec);
-    const size_t need = (size_t)(M / 2 + 1) * 2 * right->nvec * sizeof(double2);
+    // Pair sums: twice the block partials of the direct loop.
+    GQT_TRY(ws_dot(ws, (size_t)max_grid() * h->n_real * right->nvec * 8, &ds));
+    const size_t need = (size_t)(M / 2 + 1) * 2 * h->n_real * right->nvec * sizeof(double2);
     if (ws.pairs_bytes < need) {
       cudaStreamSynchronize(s);
       cudaFree(ws.pairs);

@@ -20,9 +20,10 @@ struct OpFns {
   gqt_status (*step_pair)(const Op& op, int mode, const void* t0, const void* t1, void* out,
                           const Dot& dot);
   // One step of a realisation batch (mode kDotOnly, kApply or kCheb) with moments per
-  // realisation.
+  // realisation: <left|out> (dot kDotLeft), or the pair products of a symmetric set
+  // (kDotPair: 2 nvec sums per realisation, [2v] <T_k|T_k>, [2v + 1] <T_{k-1}|T_k>).
   gqt_status (*step_multi)(const Op& op, int mode, const void* t0, const void* t1, void* out,
-                           const void* left, const MultiDot& md);
+                           const void* left, const MultiDot& md, int dot);
   gqt_status (*xop)(const Op& op, bool current, const void* in, void* out);
   // Evolution terms; out is a double2 accumulator (the FP64 state itself, or the
   // FP32 form's FP64 accumulator).
@@ -60,9 +61,9 @@ struct FormOps {
     return of(op).step_pair(op, mode, t0, t1, out, d);
   }
   gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1, void* out,
-                        const void* left, const MultiDot& md) const
+                        const void* left, const MultiDot& md, int dot = kDotLeft) const
   {
-    return of(op).step_multi(op, mode, t0, t1, out, left, md);
+    return of(op).step_multi(op, mode, t0, t1, out, left, md, dot);
   }
   gqt_status xop(const Op& op, bool current, const void* in, void* out) const
   {

@@ -176,7 +176,7 @@ struct OpImpl {
   }
 
   static gqt_status step_multi(const Op& op, int mode, const void* t0, const void* t1,
-                               void* out, const void* left, const MultiDot& md_in)
+                               void* out, const void* left, const MultiDot& md_in, int dot)
   {
     const VT2* a0 = (const VT2*)t0;
     const VT2* a1 = (const VT2*)t1;
@@ -197,6 +197,11 @@ struct OpImpl {
         constexpr int WW = decltype(wc)::value;
         if (mode == kDotOnly)
           return go(k_step_multi<VT2, V, WW, Z, A, kDotOnly, C>);
+        if (dot == kDotPair) {
+          if (mode == kApply)
+            return go(k_step_multi<VT2, V, WW, Z, A, kApply, C, kDotPair>);
+          return go(k_step_multi<VT2, V, WW, Z, A, kCheb, C, kDotPair>);
+        }
         if (mode == kApply)
           return go(k_step_multi<VT2, V, WW, Z, A, kApply, C>);
         return go(k_step_multi<VT2, V, WW, Z, A, kCheb, C>);
@@ -207,7 +212,10 @@ struct OpImpl {
       }
       return pick(std::integral_constant<int, W>{});
     }));
-    k_tile_reduce<V><<<md.n_real * V, kBlock, 0, stream()>>>(md);
+    if (dot == kDotPair && mode != kDotOnly)
+      k_tile_reduce<2 * V><<<md.n_real * 2 * V, kBlock, 0, stream()>>>(md);
+    else
+      k_tile_reduce<V><<<md.n_real * V, kBlock, 0, stream()>>>(md);
     count_launches(1);
     GQT_CUDA(cudaGetLastError());
     return GQT_OK;

@@ -1015,7 +1015,7 @@ __device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSu
 // sums are reduced over the block when the run ends and written to the block's slot
 // of that realisation; slots of realisations it never meets are zeroed.
 // k_tile_reduce then sums the blocks per realisation in fixed order.
-template <typename VT2, int V, int W, int Z, class A, int MODE, bool C>
+template <typename VT2, int V, int W, int Z, class A, int MODE, bool C, int DOT = kDotLeft>
 __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
                                                        const VT2* __restrict__ left, MultiDot md)
@@ -1024,22 +1024,27 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
   constexpr int kTps = V / W;
   constexpr int kWarps = kBlock / 32;
   constexpr bool kExact = std::is_same<A, ExactArith>::value;
-  __shared__ double sh[kWarps][V][4];
+  // Sums per realisation: V moments <left|out>, or for the pair mode of a symmetric set
+  // 2V ([2v] <T_k|T_k>, [2v + 1] <T_{k-1}|T_k>); a thread holds kSums of them.
+  static_assert(DOT == kDotLeft || (DOT == kDotPair && MODE != kDotOnly), "dot mode");
+  constexpr int kVS = DOT == kDotPair ? 2 * V : V;
+  constexpr int kSums = DOT == kDotPair ? 2 * W : W;
+  __shared__ double sh[kWarps][kVS][4];
   const int R = md.n_real;
   const size_t items_per_tile = (size_t)md.tile_sites * kTps;
-  double* slots = md.partials + (size_t)blockIdx.x * R * V * 4;
+  double* slots = md.partials + (size_t)blockIdx.x * R * kVS * 4;
   int r = 0;
   unsigned touched = 0u;  // realisations this block has written (R <= 32)
-  CSum re[W], im[W];
+  CSum re[kSums], im[kSums];
 #pragma unroll
-  for (int k = 0; k < W; ++k)
+  for (int k = 0; k < kSums; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
 
   auto flush = [&](int rr) {
     CSum br{0.0, 0.0}, bi{0.0, 0.0};
-    block_reduce_w<V, W>(re, im, br, bi, sh);
-    if (threadIdx.x < V) {
-      double* q = slots + ((size_t)rr * V + threadIdx.x) * 4;
+    block_reduce_w<kVS, kSums>(re, im, br, bi, sh);
+    if (threadIdx.x < kVS) {
+      double* q = slots + ((size_t)rr * kVS + threadIdx.x) * 4;
       q[0] = br.s;
       q[1] = br.c;
       q[2] = bi.s;
@@ -1047,7 +1052,7 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
     }
     touched |= 1u << rr;
 #pragma unroll
-    for (int k = 0; k < W; ++k)
+    for (int k = 0; k < kSums; ++k)
       re[k] = im[k] = CSum{0.0, 0.0};
   };
 
@@ -1078,11 +1083,11 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
       const int v0 = (int)(g % kTps) * W;
       const size_t base = (size_t)i * V + v0;
       double2 r2[W];
+      double2 x[W];  // T_{k-1} (the pair mode's second product)
       if constexpr (MODE == kDotOnly) {
         ldw<W>(t1 + base, r2);
       } else {
         const double p = op.pot[i];
-        double2 x[W];
         ldw<W>(t1 + base, x);
         double tr[W], ti[W];
 #pragma unroll
@@ -1131,15 +1136,30 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
         }
         stw<W>(out + base, r2);
       }
-      double2 l[W];
-      ldw<W>(left + base, l);
+      if constexpr (DOT == kDotLeft) {
+        double2 l[W];
+        ldw<W>(left + base, l);
 #pragma unroll
-      for (int k = 0; k < W; ++k) {
-        if constexpr (kExact) {
-          dot_term(re[k], im[k], MODE == kDotOnly ? r2[k] : stored(out, r2[k]), l[k]);
-        } else {
-          re[k].s = fma(r2[k].x, l[k].x, fma(r2[k].y, l[k].y, re[k].s));
-          im[k].s = fma(r2[k].y, l[k].x, fma(-r2[k].x, l[k].y, im[k].s));
+        for (int k = 0; k < W; ++k) {
+          if constexpr (kExact) {
+            dot_term(re[k], im[k], MODE == kDotOnly ? r2[k] : stored(out, r2[k]), l[k]);
+          } else {
+            re[k].s = fma(r2[k].x, l[k].x, fma(r2[k].y, l[k].y, re[k].s));
+            im[k].s = fma(r2[k].y, l[k].x, fma(-r2[k].x, l[k].y, im[k].s));
+          }
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const double2 o = stored(out, r2[k]);
+          if constexpr (kExact) {
+            dot_term(re[2 * k], im[2 * k], o, o);
+            dot_term(re[2 * k + 1], im[2 * k + 1], o, x[k]);
+          } else {
+            re[2 * k].s = fma(o.x, o.x, fma(o.y, o.y, re[2 * k].s));
+            re[2 * k + 1].s = fma(o.x, x[k].x, fma(o.y, x[k].y, re[2 * k + 1].s));
+            im[2 * k + 1].s = fma(o.y, x[k].x, fma(-o.x, x[k].y, im[2 * k + 1].s));
+          }
         }
       }
       if constexpr (kPre)
@@ -1149,8 +1169,8 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
   if (any)
     flush(r);
   // Realisations this block never met get zero sums.
-  for (int k = threadIdx.x; k < R * V * 4; k += kBlock) {
-    const int rr = k / (V * 4);
+  for (int k = threadIdx.x; k < R * kVS * 4; k += kBlock) {
+    const int rr = k / (kVS * 4);
     if (!((touched >> rr) & 1u))
       slots[k] = 0.0;
   }

@@ -222,7 +222,9 @@ gqt_status gqt_moments_device_form(const gqt_ham* h, const gqt_vec* left,
  * 2 <T_{k-1}|T_k> - mu_1). No counterpart in the reference, whose loop takes n_moments
  * steps (find_moments_chebyshev, src/sigma.cu:33-61, with left = right): same moments
  * up to rounding of order 1e-15 mu_0 per moment in the FP64 form, not bit for bit.
- * precision as in gqt_moments_form; at most 16 vectors; not for realisation batches.
+ * precision as in gqt_moments_form; the operator must be Hermitian (checked at upload,
+ * GQT_ERR_STATE otherwise); at most 16 vectors, 32 for a realisation batch (moments
+ * per realisation, as gqt_moments).
  * Outputs as gqt_moments (host) / gqt_moments_device (device, [m][vector] double2). */
 gqt_status gqt_moments_doubled(const gqt_ham* h, const gqt_vec* state, int n_moments,
                                int precision, double* mu_re, double* mu_im);

@@ -96,10 +96,31 @@ def test_doubled_limits():
     with pytest.raises(g.GqtError) as e:
         g.moments_doubled(H, X, 10)
     assert e.value.status == 1
-    B = g.Hamiltonian.batch([m, g.Model.load(fixture_dir("cubic6"))])
-    with pytest.raises(g.GqtError) as e:
-        g.moments_doubled(B, g.Vector(B.n), 10)
-    assert e.value.status == 6
+
+
+@pytest.mark.parametrize("prec,V", [(g.FP64, 4), (g.FP32, 16), (g.FP32, 32)])
+def test_doubled_batch(prec, V):
+    """Realisation batches: per-model symmetric moments from half the steps."""
+    names = ["sq16_pbc", "graphene_8x4", "cubic6", "sq12_open_vac"]
+    models = [g.Model.load(fixture_dir(n)) for n in names]
+    B = g.Hamiltonian.batch(models)
+    per = []
+    for mm in models:
+        ph = [mm.initial_state() for _ in range(V)]
+        per.append((np.stack([p[0] for p in ph]), np.stack([p[1] for p in ph])))
+    X = g.Vector.from_host(*B.scatter(per), nvec=V, precision=prec)
+    M = 151
+    dr, di = g.moments(B, X, X, M)
+    br, bi = g.moments_doubled(B, X, M)
+    assert br.shape == (len(models), V, M)
+    for r, mm in enumerate(models):
+        if prec == g.FP64:
+            assert _err((br[r], bi[r]), (dr[r], di[r])) <= ABS_FP64, r
+        else:
+            for k in range(0, V, 7):
+                d1 = g.chebyshev_summation(dr[r, k], di[r, k], mm.energy, mm.energy_max, mm.volume)
+                d2 = g.chebyshev_summation(br[r, k], bi[r, k], mm.energy, mm.energy_max, mm.volume)
+                assert np.max(np.abs(d2 - d1)) <= 1e-6 * np.max(np.abs(d1)), (r, k)
 
 
 def _run_dir(tmp_path, name, tag, extra, files=None):
