@@ -128,6 +128,9 @@ void run(Model& model, long long max_rows, int precision)
     }
   }
 
+  if (model.batch_vectors > 1 && ckpt)
+    throw InputError("batch_vectors cannot be combined with checkpoints (checkpoint_every, "
+                     "a bounded run): checkpoints are per row of one vector");
   Hamiltonian H(model);
   Vector random_state(model.number_of_atoms);
   const bool v = model.verbose;
@@ -173,7 +176,13 @@ void run(Model& model, long long max_rows, int precision)
   };
 
   const int first_vector = resumed ? start.vector : 0;
-  for (int i = first_vector; i < model.number_of_random_vectors; ++i) {
+  if (model.batch_vectors > 1) {
+    timed(v, "random vectors in groups", [&] {
+      run_vector_groups(model, H, 0, model.number_of_random_vectors, model.batch_vectors);
+    });
+  }
+  for (int i = model.batch_vectors > 1 ? model.number_of_random_vectors : first_vector;
+       i < model.number_of_random_vectors; ++i) {
     if (v)
       std::cout << "\nStarted  simulation with random vector number " << i << std::endl;
     current = i;

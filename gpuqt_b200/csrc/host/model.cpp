@@ -151,6 +151,10 @@ void Model::initialize_parameters()
       output_moments = true;
     } else if (token == "kpm_doubling") {
       kpm_doubling = true;
+    } else if (token == "batch_vectors") {
+      ss >> batch_vectors;
+      if (!ss || batch_vectors < 1)
+        bad("batch_vectors needs a number of vectors >= 1");
     } else if (token == "checkpoint_every") {
       ss >> checkpoint_every;
       if (!ss || checkpoint_every < 1)
@@ -160,7 +164,8 @@ void Model::initialize_parameters()
           "\nValid keywords include: model anderson_disorder charged_impurity "
           "vacancy_disorder calculate_vac0 calculate_vac calculate_msd calculate_spin "
           "calculate_ldos number_of_random_vectors number_of_moments energy_max seed "
-          "disorder_seed phase_seed output_moments checkpoint_every kpm_doubling");
+          "disorder_seed phase_seed output_moments checkpoint_every kpm_doubling "
+          "batch_vectors");
     }
   }
   verify_parameters();

@@ -87,32 +87,15 @@ void evolvex(Model&, int direction, real time_step_scaled, Hamiltonian& H, Vecto
 
 namespace {
 
-// Moments -> damped Chebyshev sum -> one appended row of <stem>.out; with
-// output_moments, the raw moments also go to <stem>_moments.bin.
+using gqt_host::open_out;
+
+// Moments -> one appended row of <stem>.out (gqt_host::append_row).
 void write_row(Model& model, Vector& moments, const char* stem, std::ofstream& out)
 {
   const int M = model.number_of_moments;
-  std::vector<real> re(M), im(M), row(model.number_of_energy_points);
+  std::vector<real> re(M), im(M);
   moments.copy_to_host(re.data(), im.data());
-  if (model.output_moments)
-    gqt_host::append_moments(model.input_dir + "/" + stem + "_moments.bin", M, re.data(),
-                             im.data());
-  apply_damping(model, re.data(), im.data());
-  perform_chebyshev_summation(model, re.data(), im.data(), row.data());
-  for (int n = 0; n < model.number_of_energy_points; ++n)
-    out << row[n] << " ";
-  out << std::endl;
-  if (!out)
-    gqt_host::die("Error: cannot write " + model.input_dir + "/" + stem + ".out");
-}
-
-std::ofstream open_out(Model& model, const char* stem)
-{
-  const std::string file = model.input_dir + "/" + stem + ".out";
-  std::ofstream out(file, std::ios::app);
-  if (!out.is_open())
-    gqt_host::die("Error: cannot open " + file);
-  return out;
+  gqt_host::append_row(model, re.data(), im.data(), stem, out);
 }
 
 void restore(Vector& v, const std::vector<real>& s)
@@ -133,6 +116,31 @@ void report(gqt_host::StageRun& run, int next, std::vector<Vector*> live)
 }  // namespace
 
 namespace gqt_host {
+
+void append_row(Model& model, const real* mu_re, const real* mu_im, const char* stem,
+                std::ofstream& out)
+{
+  const int M = model.number_of_moments;
+  std::vector<real> re(mu_re, mu_re + M), im(mu_im, mu_im + M), row(model.number_of_energy_points);
+  if (model.output_moments)
+    append_moments(model.input_dir + "/" + stem + "_moments.bin", M, re.data(), im.data());
+  apply_damping(model, re.data(), im.data());
+  perform_chebyshev_summation(model, re.data(), im.data(), row.data());
+  for (int n = 0; n < model.number_of_energy_points; ++n)
+    out << row[n] << " ";
+  out << std::endl;
+  if (!out)
+    die("Error: cannot write " + model.input_dir + "/" + stem + ".out");
+}
+
+std::ofstream open_out(Model& model, const char* stem)
+{
+  const std::string file = model.input_dir + "/" + stem + ".out";
+  std::ofstream out(file, std::ios::app);
+  if (!out.is_open())
+    die("Error: cannot open " + file);
+  return out;
+}
 
 // src/sigma.cu:204-239.
 void dos_stage(Model& model, Hamiltonian& H, Vector& random_state, int flag, StageRun& run)

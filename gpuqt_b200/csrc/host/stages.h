@@ -5,6 +5,7 @@
 // reference does.
 #pragma once
 
+#include <fstream>
 #include <functional>
 #include <vector>
 
@@ -25,6 +26,19 @@ struct StageRun {
   // continue with (none once the stage is complete).
   std::function<void(int next, const std::vector<Vector*>& live)> after_row;
 };
+
+// <stem>.out opened for appending (dies if it cannot be opened).
+std::ofstream open_out(Model& model, const char* stem);
+// One row from host moments: with output_moments the raw moments go to
+// <stem>_moments.bin, then Jackson damping and the Chebyshev sum at the energy grid are
+// appended to `out` in the reference's format (src/sigma.cu:204-239).
+void append_row(Model& model, const real* mu_re, const real* mu_im, const char* stem,
+                std::ofstream& out);
+// Random vectors first .. first + count - 1 as groups of up to `batch` vectors per
+// launch (para.in batch_vectors): every stage of a group runs on multi-vector states,
+// and each .out file receives the group's rows vector by vector, as the one-vector
+// run writes them. Draws the group's phases from the model's generator in order.
+void run_vector_groups(Model& model, Hamiltonian& H, int first, int count, int batch);
 
 void dos_stage(Model& model, Hamiltonian& H, Vector& random_state, int flag, StageRun& run);
 void vac0_stage(Model& model, Hamiltonian& H, Vector& random_state, StageRun& run);

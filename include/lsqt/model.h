@@ -70,6 +70,9 @@ public:
   // `kpm_doubling`: symmetric moment sets (DOS, VAC0, MSD, LDOS) from half the
   // Chebyshev steps (gqt_moments_doubled); equal to the direct moments up to rounding.
   bool kpm_doubling = false;
+  // `batch_vectors B`: random vectors run B at a time (16 or 4 per launch) through the
+  // multi-vector kernels; the .out files are those of the one-vector run.
+  int batch_vectors = 1;
   // The generator's state (with the one-time phase reseed flag), as text.
   std::string rng_state() const;
   void set_rng_state(const std::string& state);

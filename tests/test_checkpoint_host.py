@@ -39,13 +39,21 @@ def _dir(tmp_path, extra):
 
 
 def test_keywords_parse(tmp_path):
-    g.Model.load(_dir(tmp_path, "output_moments\ncheckpoint_every 3\n"))
+    g.Model.load(_dir(tmp_path, "output_moments\ncheckpoint_every 3\nkpm_doubling\n"
+                                "batch_vectors 16\n"))
     bad = str(tmp_path / "bad")
     shutil.copytree(fixture_dir("chain_z2"), bad)
     with open(os.path.join(bad, "para.in"), "a") as f:
         f.write("checkpoint_every 0\n")
     with pytest.raises(g.GqtError) as e:
         g.Model.load(bad)
+    assert e.value.status == 4
+    bad2 = str(tmp_path / "bad2")
+    shutil.copytree(fixture_dir("chain_z2"), bad2)
+    with open(os.path.join(bad2, "para.in"), "a") as f:
+        f.write("batch_vectors 0\n")
+    with pytest.raises(g.GqtError) as e:
+        g.Model.load(bad2)
     assert e.value.status == 4
 
 
