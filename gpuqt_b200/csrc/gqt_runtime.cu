@@ -423,25 +423,18 @@ void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
 bool build_codes(const Packed& P, std::vector<uint8_t>& codes, std::vector<int>& delta,
                  std::vector<double2>& hop, std::vector<double>& xx)
 {
+  // Open addressing over 1024 slots (at most GQT_MAX_CODES = 256 keys are kept, so
+  // probes stay short): one hash and a few compares per entry.
   struct Key {
     long long d;
     uint64_t hr, hi, x;
-    bool operator==(const Key& o) const
-    {
-      return d == o.d && hr == o.hr && hi == o.hi && x == o.x;
-    }
   };
-  struct KeyHash {
-    size_t operator()(const Key& k) const
-    {
-      uint64_t h = (uint64_t)k.d * 0x9e3779b97f4a7c15ull;
-      h ^= k.hr + 0x7f4a7c159e3779b9ull + (h << 6) + (h >> 2);
-      h ^= k.hi + 0x94d049bb133111ebull + (h << 6) + (h >> 2);
-      h ^= k.x + 0xbf58476d1ce4e5b9ull + (h << 6) + (h >> 2);
-      return (size_t)h;
-    }
+  constexpr int kSlots = 1024;
+  std::vector<int> slot(kSlots, -1);  // index into keys, -1 empty
+  std::vector<Key> keys;
+  auto same = [](const Key& a, const Key& b) {
+    return a.d == b.d && a.hr == b.hr && a.hi == b.hi && a.x == b.x;
   };
-  std::unordered_map<Key, int, KeyHash> dict;
   codes.assign((size_t)P.n * P.z, 0);
   for (int m = 0; m < P.z; ++m)
     for (int i = 0; i < P.n; ++i) {
@@ -451,16 +444,23 @@ bool build_codes(const Packed& P, std::vector<uint8_t>& codes, std::vector<int>&
       std::memcpy(&k.hr, &P.hop[e].x, 8);
       std::memcpy(&k.hi, &P.hop[e].y, 8);
       std::memcpy(&k.x, &P.xx[e], 8);
-      auto it = dict.find(k);
-      if (it == dict.end()) {
-        if ((int)dict.size() == GQT_MAX_CODES)
+      uint64_t h = (uint64_t)k.d * 0x9e3779b97f4a7c15ull;
+      h ^= k.hr + 0x7f4a7c159e3779b9ull + (h << 6) + (h >> 2);
+      h ^= k.hi + 0x94d049bb133111ebull + (h << 6) + (h >> 2);
+      h ^= k.x + 0xbf58476d1ce4e5b9ull + (h << 6) + (h >> 2);
+      int s = (int)(h ^ (h >> 29)) & (kSlots - 1);
+      while (slot[s] >= 0 && !same(keys[slot[s]], k))
+        s = (s + 1) & (kSlots - 1);
+      if (slot[s] < 0) {
+        if ((int)keys.size() == GQT_MAX_CODES)
           return false;
-        it = dict.emplace(k, (int)dict.size()).first;
+        slot[s] = (int)keys.size();
+        keys.push_back(k);
         delta.push_back((int)k.d);
         hop.push_back(P.hop[e]);
         xx.push_back(P.xx[e]);
       }
-      codes[e] = (uint8_t)it->second;
+      codes[e] = (uint8_t)slot[s];
     }
   return true;
 }

@@ -7,6 +7,7 @@
 // phases — so the ELL arrays, potentials and phase vectors are bit-identical.
 #include "lsqt/model.h"
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -15,6 +16,7 @@
 #include <fstream>
 #include <iostream>
 #include <sstream>
+#include <thread>
 
 #include "gpuqt.h"
 #include "lsqt/vector.h"
@@ -698,25 +700,42 @@ void Model::initialize_state_host(real* re, real* im, int orbital)
     generator.seed((unsigned)phase_seed);
     phase_reseeded = true;
   }
+  // The phases are drawn in the reference's order (one draw per phase-carrying
+  // orbital; with spin only the even orbitals carry one, src/model.cu:77-109); cos and
+  // sin of them, the bulk of the work, are evaluated over chunks in parallel threads,
+  // which gives the same values as the serial loop.
   std::uniform_real_distribution<real> phase(0, 2 * kPi);
-  if (calculate_spin) {
-    // Spin-degenerate pairs: only even orbitals carry a phase (normalised to N/2).
-    for (int n = 0; n < N; n += 2) {
-      const real p = phase(generator);
-      re[n] = std::cos(p);
-      im[n] = std::sin(p);
-      if (n + 1 < N) {
+  const int step = calculate_spin ? 2 : 1;
+  const int count = (N + step - 1) / step;
+  std::vector<real> p(count);
+  for (int k = 0; k < count; ++k)
+    p[k] = phase(generator);
+  auto fill = [&](int k0, int k1) {
+    for (int k = k0; k < k1; ++k) {
+      const int n = k * step;
+      re[n] = std::cos(p[k]);
+      im[n] = std::sin(p[k]);
+      if (step == 2 && n + 1 < N) {
         re[n + 1] = 0.0;
         im[n + 1] = 0.0;
       }
     }
-  } else {
-    for (int n = 0; n < N; ++n) {
-      const real p = phase(generator);
-      re[n] = std::cos(p);
-      im[n] = std::sin(p);
-    }
+  };
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int threads = count < (1 << 16) ? 1 : (int)std::min(16u, hw ? hw : 1u);
+  if (threads <= 1) {
+    fill(0, count);
+    return;
   }
+  std::vector<std::thread> pool;
+  const int chunk = (count + threads - 1) / threads;
+  for (int t = 0; t < threads; ++t) {
+    const int k0 = t * chunk, k1 = std::min(count, k0 + chunk);
+    if (k0 < k1)
+      pool.emplace_back(fill, k0, k1);
+  }
+  for (auto& th : pool)
+    th.join();
 }
 
 std::string Model::rng_state() const
