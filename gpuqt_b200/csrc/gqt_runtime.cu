@@ -4,7 +4,10 @@
 #include <cstdio>
 #include <cmath>
 #include <cstring>
+#include <algorithm>
+#include <atomic>
 #include <mutex>
+#include <thread>
 #include <unordered_map>
 #include <vector>
 
@@ -13,6 +16,31 @@
 #include "gqt_internal.h"
 
 namespace gqt {
+
+// f(lo, hi, chunk) over [0, n) split into contiguous chunks on host threads (one
+// chunk below 65,536 rows); returns the number of chunks. Chunk c covers rows
+// [c * per, min(n, (c + 1) * per)).
+template <class F>
+int parallel_rows(long long n, F&& f)
+{
+  const unsigned hw = std::thread::hardware_concurrency();
+  const int threads = n < (1 << 16) ? 1 : (int)std::min<unsigned>(16u, hw ? hw : 1u);
+  if (threads <= 1) {
+    f(0LL, n, 0);
+    return 1;
+  }
+  const long long per = (n + threads - 1) / threads;
+  std::vector<std::thread> pool;
+  for (int c = 0; c < threads; ++c) {
+    const long long lo = c * per, hi = std::min(n, lo + per);
+    if (lo < hi)
+      pool.emplace_back([&f, lo, hi, c] { f(lo, hi, c); });
+  }
+  for (auto& t : pool)
+    t.join();
+  return threads;
+}
+
 
 namespace {
 thread_local std::string t_error;
@@ -351,16 +379,34 @@ gqt_status validate_desc(const gqt_ell_desc* d, const char* what)
     return fail(GQT_ERR_ARG, "%s: null ELL array", what);
   if ((size_t)n * z > (size_t)1 << 40)
     return fail(GQT_ERR_ARG, "%s: n * max_neighbor too large", what);
-  for (int i = 0; i < n; ++i) {
+  // The first bad row over all chunks (the one a serial scan would report).
+  std::vector<long long> bad(17, -1);
+  parallel_rows(n, [&](long long lo, long long hi, int chunk) {
+    for (long long i = lo; i < hi; ++i) {
+      const int c = d->neighbor_number[i];
+      bool ok = c >= 0 && c <= z;
+      for (int m = 0; ok && m < c; ++m) {
+        const int j = d->neighbor_list[(size_t)i * z + m];
+        ok = j >= 0 && j < n;
+      }
+      if (!ok) {
+        bad[chunk] = i;
+        return;
+      }
+    }
+  });
+  for (long long i : bad) {
+    if (i < 0)
+      continue;
     const int c = d->neighbor_number[i];
     if (c < 0 || c > z)
-      return fail(GQT_ERR_INPUT, "%s: site %d has %d neighbours (max_neighbor %d)", what, i, c,
-                  z);
+      return fail(GQT_ERR_INPUT, "%s: site %d has %d neighbours (max_neighbor %d)", what, (int)i,
+                  c, z);
     for (int m = 0; m < c; ++m) {
       const int j = d->neighbor_list[(size_t)i * z + m];
       if (j < 0 || j >= n)
-        return fail(GQT_ERR_INPUT, "%s: site %d neighbour %d index %d out of [0, %d)", what, i,
-                    m, j, n);
+        return fail(GQT_ERR_INPUT, "%s: site %d neighbour %d index %d out of [0, %d)", what,
+                    (int)i, m, j, n);
     }
   }
   return GQT_OK;
@@ -383,9 +429,11 @@ struct Packed {
     xx.assign((size_t)n * z, 0.0);
     pot.assign(n, 0.0);
     // Rows start as padding: full length, pointing at the site itself, zero hopping.
-    for (int m = 0; m < z; ++m)
-      for (int i = 0; i < n; ++i)
-        nl[(size_t)m * n + i] = i;
+    parallel_rows(n, [&](long long lo, long long hi, int) {
+      for (int m = 0; m < z; ++m)
+        for (long long i = lo; i < hi; ++i)
+          nl[(size_t)m * n + i] = (int)i;
+    });
   }
 };
 
@@ -396,12 +444,15 @@ void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
 {
   const int n = d->n, z = d->max_neighbor;
   const double e = d->energy_max;
-  for (int i = 0; i < n; ++i) {
+  std::atomic<bool> ragged{false};
+  parallel_rows(n, [&](long long lo, long long hi, int) {
+  bool short_row = false;
+  for (int i = (int)lo; i < (int)hi; ++i) {
     const int c = d->neighbor_number[i];
     const int row = base + i;
     P.nn[row] = c;
     if (c != P.z)
-      P.uniform = false;
+      short_row = true;
     for (int m = 0; m < c; ++m) {
       const size_t src = (size_t)i * z + m, dst = (size_t)m * P.n + row;
       P.nl[dst] = base + d->neighbor_list[src];
@@ -416,6 +467,11 @@ void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
       P.nl[(size_t)m * P.n + row] = row;
     P.pot[row] = divide ? d->potential[i] / e : d->potential[i];
   }
+  if (short_row)
+    ragged = true;
+  });
+  if (ragged)
+    P.uniform = false;
 }
 
 // The dictionary of (j - i, hopping, xx) over every ELL entry, padding entries
@@ -423,45 +479,96 @@ void pack_desc(const gqt_ell_desc* d, int base, bool divide, Packed& P)
 bool build_codes(const Packed& P, std::vector<uint8_t>& codes, std::vector<int>& delta,
                  std::vector<double2>& hop, std::vector<double>& xx)
 {
-  // Open addressing over 1024 slots (at most GQT_MAX_CODES = 256 keys are kept, so
-  // probes stay short): one hash and a few compares per entry.
   struct Key {
     long long d;
     uint64_t hr, hi, x;
   };
-  constexpr int kSlots = 1024;
-  std::vector<int> slot(kSlots, -1);  // index into keys, -1 empty
-  std::vector<Key> keys;
-  auto same = [](const Key& a, const Key& b) {
-    return a.d == b.d && a.hr == b.hr && a.hi == b.hi && a.x == b.x;
-  };
-  codes.assign((size_t)P.n * P.z, 0);
-  for (int m = 0; m < P.z; ++m)
-    for (int i = 0; i < P.n; ++i) {
-      const size_t e = (size_t)m * P.n + i;
-      Key k;
-      k.d = (long long)P.nl[e] - i;
-      std::memcpy(&k.hr, &P.hop[e].x, 8);
-      std::memcpy(&k.hi, &P.hop[e].y, 8);
-      std::memcpy(&k.x, &P.xx[e], 8);
+  // At most GQT_MAX_CODES keys in first-seen order, open addressing over 1024 slots.
+  struct Dict {
+    std::vector<int> slot = std::vector<int>(1024, -1);
+    std::vector<Key> keys;
+    static uint64_t hash(const Key& k)
+    {
       uint64_t h = (uint64_t)k.d * 0x9e3779b97f4a7c15ull;
       h ^= k.hr + 0x7f4a7c159e3779b9ull + (h << 6) + (h >> 2);
       h ^= k.hi + 0x94d049bb133111ebull + (h << 6) + (h >> 2);
       h ^= k.x + 0xbf58476d1ce4e5b9ull + (h << 6) + (h >> 2);
-      int s = (int)(h ^ (h >> 29)) & (kSlots - 1);
+      return h ^ (h >> 29);
+    }
+    static bool same(const Key& a, const Key& b)
+    {
+      return a.d == b.d && a.hr == b.hr && a.hi == b.hi && a.x == b.x;
+    }
+    // The key's index, added if new; -1 once more than GQT_MAX_CODES would be kept.
+    int add(const Key& k)
+    {
+      int s = (int)(hash(k) & 1023);
       while (slot[s] >= 0 && !same(keys[slot[s]], k))
-        s = (s + 1) & (kSlots - 1);
+        s = (s + 1) & 1023;
       if (slot[s] < 0) {
         if ((int)keys.size() == GQT_MAX_CODES)
-          return false;
+          return -1;
         slot[s] = (int)keys.size();
         keys.push_back(k);
-        delta.push_back((int)k.d);
-        hop.push_back(P.hop[e]);
-        xx.push_back(P.xx[e]);
       }
-      codes[e] = (uint8_t)slot[s];
+      return slot[s];
     }
+  };
+  auto key_at = [&](int m, long long i) {
+    const size_t e = (size_t)m * P.n + i;
+    Key k;
+    k.d = (long long)P.nl[e] - i;
+    std::memcpy(&k.hr, &P.hop[e].x, 8);
+    std::memcpy(&k.hi, &P.hop[e].y, 8);
+    std::memcpy(&k.x, &P.xx[e], 8);
+    return k;
+  };
+  // Pass 1: per column and chunk of rows, the keys in first-seen order; merged in the
+  // order of a serial scan (column by column, rows ascending), the codes number the
+  // distinct entries by first appearance whatever the chunking.
+  std::atomic<bool> overflow{false};
+  Dict dict;
+  for (int m = 0; m < P.z && !overflow; ++m) {
+    std::vector<std::vector<Key>> firsts(17);
+    parallel_rows(P.n, [&](long long lo, long long hi, int chunk) {
+      Dict local;
+      for (long long i = lo; i < hi; ++i)
+        if (local.add(key_at(m, i)) < 0) {
+          overflow = true;
+          return;
+        }
+      firsts[chunk] = std::move(local.keys);
+    });
+    for (auto& f : firsts)
+      for (const Key& k : f)
+        if (!overflow && dict.add(k) < 0)
+          overflow = true;
+  }
+  if (overflow)
+    return false;
+  for (const Key& k : dict.keys) {
+    double2 h;
+    double x;
+    std::memcpy(&h.x, &k.hr, 8);
+    std::memcpy(&h.y, &k.hi, 8);
+    std::memcpy(&x, &k.x, 8);
+    delta.push_back((int)k.d);
+    hop.push_back(h);
+    xx.push_back(x);
+  }
+  // Pass 2: every entry's code (lookups only).
+  codes.assign((size_t)P.n * P.z, 0);
+  parallel_rows(P.n, [&](long long lo, long long hi, int) {
+    Dict& d = dict;
+    for (int m = 0; m < P.z; ++m)
+      for (long long i = lo; i < hi; ++i) {
+        const Key k = key_at(m, i);
+        int s = (int)(Dict::hash(k) & 1023);
+        while (!Dict::same(d.keys[d.slot[s]], k))
+          s = (s + 1) & 1023;
+        codes[(size_t)m * P.n + i] = (uint8_t)d.slot[s];
+      }
+  });
   return true;
 }
 
@@ -472,7 +579,9 @@ bool is_hermitian(const Packed& P)
 {
   auto row_len = [&](int i) { return P.uniform ? P.z : P.nn[i]; };
   auto entry = [&](int i, int m) { return (size_t)m * P.n + i; };
-  for (int i = 0; i < P.n; ++i) {
+  std::atomic<bool> broken{false};
+  parallel_rows(P.n, [&](long long lo, long long hi, int) {
+  for (int i = (int)lo; i < (int)hi && !broken; ++i) {
     const int ci = row_len(i);
     for (int m = 0; m < ci; ++m) {
       const int j = P.nl[entry(i, m)];
@@ -497,14 +606,15 @@ bool is_hermitian(const Packed& P)
         }
       if (j == i) {  // an entry to the site itself must be real
         if (std::fabs(si) > 1e-12 * mag)
-          return false;
+          broken = true;
         continue;
       }
       if (std::fabs(sr - tr) > 1e-12 * mag || std::fabs(si + ti) > 1e-12 * mag)
-        return false;
+        broken = true;
     }
   }
-  return true;
+  });
+  return !broken;
 }
 
 gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
