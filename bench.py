@@ -11,7 +11,7 @@ over all ranks (sites x moments x steps / max-over-ranks device time).
 Also reported: the roofline of the dominant kernel (the fused Chebyshev step + moment
 partial sums), the same metric end to end through the public API with host buffers
 (e2e), the plain FP64 rate on the reference's ELL arrays, the FP32-storage batched
-form (16 vectors per launch) with its DOS error against FP64 and its speed-up over
+form (16 and 32 vectors per launch) with its DOS error against FP64 and its speed-up over
 both FP64 rates, the realisation batch, the Bessel evolution cost, and the
 reference's CPU path timed on this host's cores (cpu_baseline).
 
@@ -386,7 +386,7 @@ def run_ours(args):
 
 
 def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
-    """FP32-storage forms on the same lattice: 1 and 16 vectors per launch, with the
+    """FP32-storage forms on the same lattice: 1, 16 and 32 vectors per launch, with the
     DOS error of vector 0 against its FP64 moments; and the Bessel evolution."""
     n, M = m.n, m.n_moments
     out = {}
@@ -395,7 +395,7 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
     r64, i64 = g.moments(H, x64, x64, M)
     fp64_rate = None
     coded = H.format == g.FORMAT_CODED
-    for V in (1, 16):
+    for V in (1, 16, 32):
         vecs = [phi] + [m.initial_state() for _ in range(V - 1)]
         re = np.stack([v[0] for v in vecs])
         im = np.stack([v[1] for v in vecs])
