@@ -6,7 +6,8 @@ them, storing its raw results at full precision (ref/<name>/). It also copies th
 reference's shipped example outputs used as golden vectors (examples/...). Needs the
 reference checkout; run it here, commit the results:
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py                  # everything
+    python tests/golden/make_golden.py --examples-only  # only the shipped examples
 """
 from __future__ import annotations
 
@@ -214,6 +215,20 @@ def main() -> None:
                     shutil.copy(p, os.path.join(o, f))
         print("fixture", name, "n =", ell.n)
 
+    copy_examples()
+    shutil.rmtree(tmp)
+
+
+def copy_examples() -> None:
+    """The reference's shipped example inputs and outputs used as golden vectors."""
+    # examples/review/graphene/vacancy: 19.8M sites with 200,000 vacancies; its dos.out
+    # holds 10 one-vector rows from unseeded runs (compared statistically).
+    src = os.path.join(REF_EXAMPLES, "review", "graphene", "vacancy")
+    dst = os.path.join(HERE, "examples", "review_graphene_vacancy")
+    os.makedirs(dst, exist_ok=True)
+    for f in ("para.in", "lattice.in", "energy.in", "time_step.in", "dos.out"):
+        shutil.copy(os.path.join(src, f), os.path.join(dst, f))
+    print("example review/graphene/vacancy")
     # Shipped example outputs of the reference (examples/fan2018cpc/lattice/*).
     for ex in ("diffusive", "localized"):
         src = os.path.join(REF_EXAMPLES, "fan2018cpc", "lattice", ex)
@@ -224,8 +239,10 @@ def main() -> None:
             if os.path.exists(os.path.join(src, f)):
                 shutil.copy(os.path.join(src, f), os.path.join(dst, f))
         print("example", ex)
-    shutil.rmtree(tmp)
 
 
 if __name__ == "__main__":
-    main()
+    if "--examples-only" in sys.argv:
+        copy_examples()
+    else:
+        main()
