@@ -68,11 +68,20 @@ gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out)
     ws.dot.blocks = (int)need;  // capacity in doubles
   }
   if (!ws.dot.counter) {
-    GQT_CUDA(cudaMalloc(&ws.dot.counter, sizeof(unsigned)));
-    GQT_CUDA(cudaMemset(ws.dot.counter, 0, sizeof(unsigned)));
+    GQT_CUDA(cudaMalloc(&ws.dot.counter, 2 * sizeof(unsigned)));
+    GQT_CUDA(cudaMemset(ws.dot.counter, 0, 2 * sizeof(unsigned)));
   }
   *out = &ws.dot;
   return GQT_OK;
+}
+
+// The slab of deferred block partials ([window][grid][results][4] doubles, after the
+// immediate partials) stays within 32 MiB.
+int defer_window(int results)
+{
+  const size_t per = (size_t)max_grid() * results * 4 * sizeof(double);
+  const size_t w = ((size_t)32 << 20) / per;
+  return (int)(w < 8 ? 8 : (w > 256 ? 256 : w));
 }
 
 namespace {
@@ -173,6 +182,67 @@ int evolvex_label(int m, int direction)
   return 2;
 }
 
+// Moment launches whose grid stage is deferred (Dot::defer): the j-th step of a window
+// writes its block partials to slab row j (rows start one immediate-partials stride into
+// the scratch), and after `len` steps, or the last one, one k_slab_combine launch turns
+// the window's rows into its moments. The outputs of consecutive moments are
+// `results` double2 apart. A step then ends without the arrival counter and the
+// last block's serial combination, which otherwise closes every launch.
+struct Deferred {
+  DotScratch* ds;
+  int results;
+  int len;
+  size_t stride;  // doubles per row
+  double2* first = nullptr;
+  int used = 0;
+
+  Deferred(DotScratch* d, int r)
+      : ds(d), results(r), len(defer_window(r)), stride((size_t)max_grid() * r * 4)
+  {
+  }
+
+  Dot next(double2* mu)
+  {
+    if (used == 0)
+      first = mu;
+    return Dot{ds->partials + (size_t)(1 + used++) * stride, ds->counter, mu, 1};
+  }
+
+  gqt_status flush(bool last)
+  {
+    if (used == 0 || (!last && used < len))
+      return GQT_OK;
+    const double* slab = ds->partials + stride;
+    cudaStream_t s = stream();
+    switch (results) {
+      case 1:
+        k_slab_combine<1><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      case 2:
+        k_slab_combine<2><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      case 4:
+        k_slab_combine<4><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      case 8:
+        k_slab_combine<8><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      case 16:
+        k_slab_combine<16><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      case 32:
+        k_slab_combine<32><<<used, kBlock, 0, s>>>(slab, stride, ds->counter, first);
+        break;
+      default:
+        return fail(GQT_ERR_ARG, "deferred moments: %d sums per moment", results);
+    }
+    count_launches(1);
+    GQT_CUDA(cudaGetLastError());
+    used = 0;
+    return GQT_OK;
+  }
+};
+
 // The launch sequence of the moment loop (src/sigma.cu:33-61) on the current stream.
 // Buffers: T_0 = right (read only), T_1 -> A, then T_m overwrites T_{m-2} in place.
 gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* left,
@@ -210,10 +280,12 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
   GQT_TRY(f->step(op, kApply, nullptr, right->data, A, left->data, &d));
   const void* prev = right->data;  // T_{m-2}
   void* cur = A;                   // T_{m-1}
+  Deferred df(ds, V);
   for (int m = 2; m < M; ++m) {
     void* out = (prev == right->data) ? B : (void*)prev;
-    d.mu = mu + (size_t)m * V;
-    GQT_TRY(f->step(op, kCheb, prev, cur, out, left->data, &d));
+    const Dot e = df.next(mu + (size_t)m * V);
+    GQT_TRY(f->step(op, kCheb, prev, cur, out, left->data, &e));
+    GQT_TRY(df.flush(m == M - 1));
     prev = cur;
     cur = out;
   }
@@ -264,10 +336,12 @@ gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_ve
     GQT_TRY(f->step_pair(op, kApply, nullptr, phi->data, A, d));
     const void* prev = phi->data;
     void* cur = A;
+    Deferred df(ds, 2 * V);
     for (int k = 2; k <= K; ++k) {
       void* out = (prev == phi->data) ? B : (void*)prev;
-      d.mu = pairs + (size_t)k * 2 * V;
-      GQT_TRY(f->step_pair(op, kCheb, prev, cur, out, d));
+      const Dot e = df.next(pairs + (size_t)k * 2 * V);
+      GQT_TRY(f->step_pair(op, kCheb, prev, cur, out, e));
+      GQT_TRY(df.flush(k == K));
       prev = cur;
       cur = out;
     }
@@ -516,8 +590,10 @@ static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const g
   const size_t bytes = right->bytes;
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
-  // Block partials: [grid][R][V][4] doubles for a batch, [grid][V][4] otherwise.
-  GQT_TRY(ws_dot(ws, (size_t)max_grid() * h->n_real * right->nvec * 4, ds));
+  // Block partials: [grid][R][V][4] doubles for a batch; [grid][V][4] otherwise, followed
+  // by the slab of a window of deferred moments.
+  const size_t rows = h->n_real > 1 ? 1 : 1 + (size_t)defer_window(right->nvec);
+  GQT_TRY(ws_dot(ws, rows * max_grid() * h->n_real * right->nvec * 4, ds));
   return GQT_OK;
 }
 
@@ -539,8 +615,9 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
                   "%s: the operator is not Hermitian (the doubling identity needs H = H^+)", w);
     if (h->n_real == 1 && right->nvec > 16)
       return fail(GQT_ERR_ARG, "%s: at most 16 vectors (got %d)", w, right->nvec);
-    // Pair sums: twice the block partials of the direct loop.
-    GQT_TRY(ws_dot(ws, (size_t)max_grid() * h->n_real * right->nvec * 8, &ds));
+    // Pair sums: twice the block partials of the direct loop (and of its slab).
+    const size_t rows = h->n_real > 1 ? 1 : 1 + (size_t)defer_window(2 * right->nvec);
+    GQT_TRY(ws_dot(ws, rows * max_grid() * h->n_real * right->nvec * 8, &ds));
     const size_t need = (size_t)(M / 2 + 1) * 2 * h->n_real * right->nvec * sizeof(double2);
     if (ws.pairs_bytes < need) {
       cudaStreamSynchronize(s);
@@ -577,6 +654,7 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
       st = pair ? moment_launches_pair(h, f, right, M, (double2*)mu_dev, ws.pairs, A, B, ds)
                 : moment_launches(h, f, left, right, M, (double2*)mu_dev, A, B, ds);
       // Captured launches run later, when the graph is launched.
+      ws.graph_launches[key] = gqt_launch_count() - before;
       gqt_reset_launch_count();
       count_launches(before);
       e = cudaStreamEndCapture(ws.capture_stream, &g);
@@ -602,7 +680,7 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
   GQT_CUDA(cudaEventRecord(ws.ev_in, s));
   GQT_CUDA(cudaStreamWaitEvent(ws.capture_stream, ws.ev_in, 0));
   GQT_CUDA(cudaGraphLaunch(it->second, ws.capture_stream));
-  count_launches((uint64_t)M);
+  count_launches(ws.graph_launches[key]);
   GQT_CUDA(cudaEventRecord(ws.ev_out, ws.capture_stream));
   GQT_CUDA(cudaStreamWaitEvent(s, ws.ev_out, 0));
   return GQT_OK;

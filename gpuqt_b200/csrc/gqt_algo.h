@@ -30,6 +30,7 @@ struct Workspace {
   // loop 0 the direct one, 1 the symmetric (pair) one.
   using GraphKey = std::tuple<const void*, const void*, int, void*, int, int, int>;
   std::map<GraphKey, cudaGraphExec_t> graphs;
+  std::map<GraphKey, uint64_t> graph_launches;  // kernel launches one replay runs
   ~Workspace();
 };
 
@@ -38,5 +39,7 @@ Workspace* new_workspace();
 // The i-th temporary vector of a form (n * nvec elements of elem bytes).
 gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i, void** out);
 gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out);
+// Moments per window of deferred grid stages for `results` sums per moment.
+int defer_window(int results);
 
 }  // namespace gqt

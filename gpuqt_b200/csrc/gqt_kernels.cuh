@@ -54,8 +54,11 @@ struct Op {
 
 struct Dot {
   double* partials;  // [gridDim.x][V][4]
-  unsigned* counter;
+  unsigned* counter; // [0] arrival counter, [1] grid of the deferred launches
   double2* mu;       // this moment's V results
+  // 1: the block writes its partials and leaves; k_slab_combine combines them later
+  // in the same order (block 0 records gridDim.x in counter[1]).
+  int defer;
 };
 
 // ------------------------------------------------------------------ operator entries
@@ -249,10 +252,70 @@ __device__ __forceinline__ CSum shfl_xor(const CSum& a, int off)
   return b;
 }
 
+// The grid stage of a moment: one block combines the partials of nblocks blocks
+// ([block][V][4]) in fixed block order and writes mu[v] for v < V. Thread t sums
+// blocks t/V, t/V + kBlock/V, ... of vector t % V; lanes and warps then merge in a
+// fixed pattern, so the result depends only on nblocks and the partials. Must be
+// reached by every thread of the block.
+template <int V>
+__device__ __forceinline__ void grid_combine(const double* partials, int nblocks, double2* mu,
+                                             double (&sh)[kBlock / 32][V][4])
+{
+  constexpr int kWarps = kBlock / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int v = threadIdx.x % V;
+  constexpr int kStride = kBlock / V;
+  CSum r{0.0, 0.0}, i{0.0, 0.0};
+  int b = threadIdx.x / V;
+  // Four blocks' partials are loaded before they are merged (in block order), so the
+  // L2 round trips overlap.
+  for (; b + 3 * kStride < nblocks; b += 4 * kStride) {
+    double q[4][4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const double* p = partials + ((size_t)(b + u * kStride) * V + v) * 4;
+#pragma unroll
+      for (int k = 0; k < 4; ++k)
+        q[u][k] = __ldcg(p + k);
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      csum_merge(r, CSum{q[u][0], q[u][1]});
+      csum_merge(i, CSum{q[u][2], q[u][3]});
+    }
+  }
+  for (; b < nblocks; b += kStride) {
+    const double* p = partials + ((size_t)b * V + v) * 4;
+    csum_merge(r, CSum{__ldcg(p + 0), __ldcg(p + 1)});
+    csum_merge(i, CSum{__ldcg(p + 2), __ldcg(p + 3)});
+  }
+#pragma unroll
+  for (int off = 16; off >= V; off >>= 1) {
+    csum_merge(r, shfl_xor(r, off));
+    csum_merge(i, shfl_xor(i, off));
+  }
+  __syncthreads();
+  if (lane < V) {
+    sh[warp][lane][0] = r.s;
+    sh[warp][lane][1] = r.c;
+    sh[warp][lane][2] = i.s;
+    sh[warp][lane][3] = i.c;
+  }
+  __syncthreads();
+  if (threadIdx.x < V) {
+    CSum rr{sh[0][v][0], sh[0][v][1]}, ii{sh[0][v][2], sh[0][v][3]};
+    for (int w = 1; w < kWarps; ++w) {
+      csum_merge(rr, CSum{sh[w][v][0], sh[w][v][1]});
+      csum_merge(ii, CSum{sh[w][v][2], sh[w][v][3]});
+    }
+    mu[v] = make_double2(__dadd_rn(rr.s, rr.c), __dadd_rn(ii.s, ii.c));
+  }
+}
+
 // Combine per-thread partials across the block, then across the grid (last block,
-// fixed order), and write dot.mu[v] for v < V. A thread holds the sums of W
-// consecutive vectors v0 .. v0+W-1, v0 = (lane % (V/W)) * W. Must be reached by every
-// thread of the block.
+// fixed order, or k_slab_combine later when dot.defer is set), and write dot.mu[v] for
+// v < V. A thread holds the sums of W consecutive vectors v0 .. v0+W-1,
+// v0 = (lane % (V/W)) * W. Must be reached by every thread of the block.
 template <int V, int W>
 __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const Dot& dot)
 {
@@ -294,8 +357,15 @@ __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const
     p[1] = r.c;
     p[2] = i.s;
     p[3] = i.c;
-    __threadfence();
+    if (dot.defer) {
+      if (blockIdx.x == 0 && v == 0)
+        dot.counter[1] = gridDim.x;
+    } else {
+      __threadfence();
+    }
   }
+  if (dot.defer)
+    return;  // uniform: a launch parameter
   __syncthreads();
   if (threadIdx.x == 0)
     is_last = (atomicAdd(dot.counter, 1u) == gridDim.x - 1) ? 1u : 0u;
@@ -303,55 +373,7 @@ __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const
   if (!is_last)
     return;
   __threadfence();
-
-  // Last block: thread t sums blocks t/V, t/V + kBlock/V, ... of vector t % V.
-  const int v = threadIdx.x % V;
-  constexpr int kStride = kBlock / V;
-  CSum r{0.0, 0.0}, i{0.0, 0.0};
-  int b = threadIdx.x / V;
-  // Four blocks' partials are loaded before they are merged (in block order), so the
-  // L2 round trips overlap.
-  for (; b + 3 * kStride < (int)gridDim.x; b += 4 * kStride) {
-    double q[4][4];
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const double* p = dot.partials + ((size_t)(b + u * kStride) * V + v) * 4;
-#pragma unroll
-      for (int k = 0; k < 4; ++k)
-        q[u][k] = __ldcg(p + k);
-    }
-#pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      csum_merge(r, CSum{q[u][0], q[u][1]});
-      csum_merge(i, CSum{q[u][2], q[u][3]});
-    }
-  }
-  for (; b < (int)gridDim.x; b += kStride) {
-    const double* p = dot.partials + ((size_t)b * V + v) * 4;
-    csum_merge(r, CSum{__ldcg(p + 0), __ldcg(p + 1)});
-    csum_merge(i, CSum{__ldcg(p + 2), __ldcg(p + 3)});
-  }
-#pragma unroll
-  for (int off = 16; off >= V; off >>= 1) {
-    csum_merge(r, shfl_xor(r, off));
-    csum_merge(i, shfl_xor(i, off));
-  }
-  __syncthreads();
-  if (lane < V) {
-    sh[warp][lane][0] = r.s;
-    sh[warp][lane][1] = r.c;
-    sh[warp][lane][2] = i.s;
-    sh[warp][lane][3] = i.c;
-  }
-  __syncthreads();
-  if (threadIdx.x < V) {
-    CSum rr{sh[0][v][0], sh[0][v][1]}, ii{sh[0][v][2], sh[0][v][3]};
-    for (int w = 1; w < kWarps; ++w) {
-      csum_merge(rr, CSum{sh[w][v][0], sh[w][v][1]});
-      csum_merge(ii, CSum{sh[w][v][2], sh[w][v][3]});
-    }
-    dot.mu[v] = make_double2(__dadd_rn(rr.s, rr.c), __dadd_rn(ii.s, ii.c));
-  }
+  grid_combine<V>(dot.partials, (int)gridDim.x, dot.mu, sh);
   if (threadIdx.x == 0)
     *dot.counter = 0u;  // ready for the next launch on this stream
 }
@@ -1525,6 +1547,21 @@ __global__ void __launch_bounds__(kBlock) k_segment_sum(const double2* __restric
     }
     out[blockIdx.x] = make_double2(__dadd_rn(r.s, r.c), __dadd_rn(i.s, i.c));
   }
+}
+
+// Grid stage of a window of deferred moments (Dot::defer): block b combines the
+// partials of moment b (slab + b * stride, counter[1] blocks) into mu + b * V, in the
+// order of the last-block stage of dot_finish_w, so a deferred moment is bit-identical
+// to an immediate one.
+template <int V>
+__global__ void __launch_bounds__(kBlock) k_slab_combine(const double* __restrict__ slab,
+                                                         size_t stride,
+                                                         const unsigned* __restrict__ counter,
+                                                         double2* mu)
+{
+  __shared__ double sh[kBlock / 32][V][4];
+  grid_combine<V>(slab + (size_t)blockIdx.x * stride, (int)counter[1],
+                  mu + (size_t)blockIdx.x * V, sh);
 }
 
 // Moments of a symmetric set from its pair products: slot k (1 <= k <= K) of `pairs`
