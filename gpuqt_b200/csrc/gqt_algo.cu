@@ -22,6 +22,7 @@ Workspace::~Workspace()
   cudaFree(dot.partials);
   cudaFree(dot.counter);
   cudaFree(mu);
+  cudaFreeHost(mu_host);
   cudaFree(pairs);
   if (ev_in)
     cudaEventDestroy(ev_in);
@@ -807,9 +808,18 @@ static gqt_status moments_host(const gqt_ham* h, const gqt_vec* left, const gqt_
       cudaGraphExecDestroy(kv.second);
     ws.graphs.clear();
   }
+  // The moments come back through a pinned buffer (a plain DMA), not the driver's
+  // staging path for pageable memory.
+  if (ws.mu_host_bytes < need) {
+    cudaFreeHost(ws.mu_host);
+    ws.mu_host = nullptr;
+    ws.mu_host_bytes = 0;
+    GQT_CUDA(cudaMallocHost(&ws.mu_host, need));
+    ws.mu_host_bytes = need;
+  }
   GQT_TRY(moments_form_run(h, left, right, M, precision, ws.mu, pair, w));
-  std::vector<double2> host((size_t)M * V);
-  GQT_CUDA(cudaMemcpyAsync(host.data(), ws.mu, need, cudaMemcpyDeviceToHost, stream()));
+  const double2* host = ws.mu_host;
+  GQT_CUDA(cudaMemcpyAsync(ws.mu_host, ws.mu, need, cudaMemcpyDeviceToHost, stream()));
   GQT_CUDA(cudaStreamSynchronize(stream()));
   for (int k = 0; k < V; ++k)
     for (int m = 0; m < M; ++m) {

@@ -22,6 +22,8 @@ struct Workspace {
   DotScratch dot;          // block partials + arrival counter of fused moment launches
   double2* mu = nullptr;   // device moments for the host-returning entry points
   size_t mu_bytes = 0;
+  double2* mu_host = nullptr;  // pinned copy of mu read by those entry points
+  size_t mu_host_bytes = 0;
   cudaStream_t capture_stream = nullptr;  // used when the caller's stream is the legacy one
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   double2* pairs = nullptr;  // pair products of the symmetric moment loop

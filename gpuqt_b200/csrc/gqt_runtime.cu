@@ -256,6 +256,36 @@ extern "C" gqt_status gqt_vec_info(const gqt_vec* v, int* n, int* nvec, int* pre
 
 extern "C" void* gqt_vec_data(gqt_vec* v) { return v ? v->data : nullptr; }
 
+// Upload and download staging comes from a pool of this library's own that keeps its
+// memory mapped between calls (release threshold: never). The default pool returns
+// freed memory to the system at every synchronisation, so a loop of uploads would map
+// and unmap its staging pages each time.
+static gqt_status stage_alloc(double** p, size_t bytes)
+{
+  static std::mutex mu;
+  static std::unordered_map<int, cudaMemPool_t> pools;
+  int dev = 0;
+  GQT_CUDA(cudaGetDevice(&dev));
+  cudaMemPool_t pool;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(dev);
+    if (it == pools.end()) {
+      cudaMemPoolProps props = {};
+      props.allocType = cudaMemAllocationTypePinned;
+      props.location.type = cudaMemLocationTypeDevice;
+      props.location.id = dev;
+      GQT_CUDA(cudaMemPoolCreate(&pool, &props));
+      uint64_t keep = UINT64_MAX;
+      GQT_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+      it = pools.emplace(dev, pool).first;
+    }
+    pool = it->second;
+  }
+  GQT_CUDA(cudaMallocFromPoolAsync((void**)p, bytes, pool, t_stream));
+  return GQT_OK;
+}
+
 extern "C" gqt_status gqt_vec_upload(gqt_vec* v, const double* re, const double* im)
 {
   GQT_TRY(check_vec(v, "gqt_vec_upload"));
@@ -266,7 +296,7 @@ extern "C" gqt_status gqt_vec_upload(gqt_vec* v, const double* re, const double*
     return GQT_ERR_ARG;
   const size_t count = (size_t)v->n * v->nvec;
   double* stage = nullptr;
-  GQT_CUDA(cudaMallocAsync((void**)&stage, 2 * count * sizeof(double), t_stream));
+  GQT_TRY(stage_alloc(&stage, 2 * count * sizeof(double)));
   gqt_status st = GQT_OK;
   cudaError_t e = cudaMemcpyAsync(stage, re, count * sizeof(double), cudaMemcpyHostToDevice,
                                   t_stream);
@@ -291,18 +321,36 @@ extern "C" gqt_status gqt_vec_download(const gqt_vec* v, double* re, double* im)
     return GQT_ERR_ARG;
   const size_t count = (size_t)v->n * v->nvec;
   double* stage = nullptr;
-  GQT_CUDA(cudaMallocAsync((void**)&stage, 2 * count * sizeof(double), t_stream));
+  GQT_TRY(stage_alloc(&stage, 2 * count * sizeof(double)));
   gqt_status st = f->deinterleave(v->n, v->nvec, v->data, stage, stage + count);
   if (st == GQT_OK) {
-    cudaError_t e = cudaMemcpyAsync(re, stage, count * sizeof(double), cudaMemcpyDeviceToHost,
-                                    t_stream);
+    // Through a pinned bounce buffer (one per device, grown as needed): a plain DMA and
+    // a host copy, not the driver's staging path for pageable memory.
+    static std::mutex mu;
+    static std::unordered_map<int, std::pair<double*, size_t>> bounce;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto& b = bounce[dev];
+    const size_t bytes = 2 * count * sizeof(double);
+    cudaError_t e = cudaSuccess;
+    if (b.second < bytes) {
+      cudaFreeHost(b.first);
+      b = {nullptr, 0};
+      e = cudaMallocHost((void**)&b.first, bytes);
+      if (e == cudaSuccess)
+        b.second = bytes;
+    }
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(im, stage + count, count * sizeof(double), cudaMemcpyDeviceToHost,
-                          t_stream);
+      e = cudaMemcpyAsync(b.first, stage, bytes, cudaMemcpyDeviceToHost, t_stream);
     if (e == cudaSuccess)
       e = cudaStreamSynchronize(t_stream);
-    if (e != cudaSuccess)
+    if (e == cudaSuccess) {
+      std::memcpy(re, b.first, count * sizeof(double));
+      std::memcpy(im, b.first + count, count * sizeof(double));
+    } else {
       st = cuda_fail(e, "download", __FILE__, __LINE__);
+    }
   }
   cudaFreeAsync(stage, t_stream);
   return st;
