@@ -324,31 +324,35 @@ extern "C" gqt_status gqt_vec_download(const gqt_vec* v, double* re, double* im)
   GQT_TRY(stage_alloc(&stage, 2 * count * sizeof(double)));
   gqt_status st = f->deinterleave(v->n, v->nvec, v->data, stage, stage + count);
   if (st == GQT_OK) {
-    // Through a pinned bounce buffer (one per device, grown as needed): a plain DMA and
-    // a host copy, not the driver's staging path for pageable memory.
+    // Through a pinned bounce buffer of kBounce doubles per device, chunk by chunk: a
+    // plain DMA and a host copy, not the driver's staging path for pageable memory,
+    // with the pinned memory bounded whatever the vector size.
+    constexpr size_t kBounce = (size_t)1 << 20;  // 8 MiB
     static std::mutex mu;
-    static std::unordered_map<int, std::pair<double*, size_t>> bounce;
+    static std::unordered_map<int, double*> bounce;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
-    auto& b = bounce[dev];
-    const size_t bytes = 2 * count * sizeof(double);
+    double*& b = bounce[dev];
     cudaError_t e = cudaSuccess;
-    if (b.second < bytes) {
-      cudaFreeHost(b.first);
-      b = {nullptr, 0};
-      e = cudaMallocHost((void**)&b.first, bytes);
-      if (e == cudaSuccess)
-        b.second = bytes;
+    if (!b)
+      e = cudaMallocHost((void**)&b, kBounce * sizeof(double));
+    for (int part = 0; part < 2 && e == cudaSuccess; ++part) {
+      const double* src = stage + part * count;
+      double* dst = part ? im : re;
+      for (size_t off = 0; off < count && e == cudaSuccess; off += kBounce) {
+        const size_t len = count - off < kBounce ? count - off : kBounce;
+        e = cudaMemcpyAsync(b, src + off, len * sizeof(double), cudaMemcpyDeviceToHost,
+                            t_stream);
+        if (e == cudaSuccess)
+          e = cudaStreamSynchronize(t_stream);
+        if (e == cudaSuccess)
+          std::memcpy(dst + off, b, len * sizeof(double));
+      }
     }
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(b.first, stage, bytes, cudaMemcpyDeviceToHost, t_stream);
-    if (e == cudaSuccess)
-      e = cudaStreamSynchronize(t_stream);
-    if (e == cudaSuccess) {
-      std::memcpy(re, b.first, count * sizeof(double));
-      std::memcpy(im, b.first + count, count * sizeof(double));
-    } else {
+    if (e != cudaSuccess) {
+      if (!b)
+        bounce.erase(dev);
       st = cuda_fail(e, "download", __FILE__, __LINE__);
     }
   }
