@@ -24,7 +24,11 @@ LIB_PATH = os.path.join(HERE, "_build", "liblsqt_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_DRIVER = os.path.join(REF_DIR, "ref_driver")
 REF_LSQT = os.path.join(REF_DIR, "lsqt_cpu")
-REFERENCE_SRC = "/root/reference/src"
+# The reference checkout: $GQT_REFERENCE, else a `reference` directory beside this
+# repository. Only the build of _ref/ reads it; the GPU host never does.
+REFERENCE_ROOT = os.environ.get("GQT_REFERENCE") or os.path.join(
+    os.path.dirname(os.path.dirname(HERE)), "reference")
+REFERENCE_SRC = os.path.join(REFERENCE_ROOT, "src")
 
 _lib = None
 
@@ -38,7 +42,8 @@ def build(ref: bool | None = None) -> None:
     if ref is None:
         ref = os.path.isdir(REFERENCE_SRC)
     if ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF_SRC={REFERENCE_SRC}"],
+                       check=True)
 
 
 def have_ref() -> bool:

@@ -23,7 +23,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import oracle  # noqa: E402
 
-REF_EXAMPLES = "/root/reference/examples"
+REF_EXAMPLES = os.path.join(oracle.REFERENCE_ROOT, "examples")
 INPUTS = os.path.join(HERE, "inputs")
 OUT = os.path.join(HERE, "ref")
 

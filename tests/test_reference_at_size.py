@@ -1,0 +1,114 @@
+"""Parity with the reference's own build at the benchmark sizes (fixtures of
+tests/golden/make_golden_large.py):
+
+  graphene2m  2,097,152 sites, z = 3: all 3000 DOS moments, and the MSD moment sets of
+              2 Bessel steps of 1 fs (evolve and evolvex at size)
+  graphene4m  4,194,304 sites: the first 500 DOS moments
+  cubic256    16,777,216 sites, z = 6: the first 200 DOS moments
+
+The host model builder must reproduce the reference's ELL arrays, hoppings, xx and
+Anderson potentials bit for bit (SHA-256 of each array; CPU), and the FP64 form every
+moment to 1e-12 relative (GPU), in both operator formats. At these sizes every thread
+of the step kernels runs several grid-stride iterations, which the small fixtures never
+reach, so the hand-over between elements is checked against the reference itself."""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import gpuqt_b200 as g
+from conftest import REF, fixture_dir, ref_moments, ref_npz
+
+LARGE = ["graphene2m", "graphene4m", "cubic256"]
+REL_FP64 = 1e-12  # per moment, |mu - mu_ref| / |mu_ref| (complex modulus)
+
+
+def _meta(name):
+    with open(os.path.join(REF, name, "model.json")) as f:
+        return json.load(f)
+
+
+def _digests(m):
+    """SHA-256 of the model's ELL arrays in the reference's host layout ([i * z + m]),
+    entries past a row's length zeroed (as the fixture generator stores them)."""
+    n, z = m.n, m.max_neighbor
+    nn = np.ascontiguousarray(m.neighbor_number, dtype=np.int32)
+    mask = np.arange(z)[None, :] < nn[:, None]
+
+    def h(a, dtype):
+        a = np.ascontiguousarray(a, dtype=dtype).reshape(n, -1).copy()
+        if a.shape[1] == z:
+            a[~mask] = 0
+        return hashlib.sha256(a.tobytes()).hexdigest()
+
+    return {"neighbor_number": h(nn, np.int32), "neighbor_list": h(m.neighbor_list, np.int32),
+            "potential": h(m.potential, np.float64),
+            "hopping_real": h(m.hopping_real, np.float64),
+            "hopping_imag": h(m.hopping_imag, np.float64), "xx": h(m.xx, np.float64)}
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("name", LARGE)
+def test_model_matches_reference_build_at_size(name):
+    meta = _meta(name)
+    m = g.Model.load(fixture_dir(name))
+    assert (m.n, m.max_neighbor) == (meta["n"], meta["z"])
+    assert m.energy_max == meta["energy_max"] and m.volume == meta["volume"]
+    assert _digests(m) == meta["sha256"]
+
+
+def _rel(mr, mi, rr, ri):
+    return float(np.max(np.hypot(mr - rr, mi - ri) / np.hypot(rr, ri)))
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+@pytest.mark.parametrize("name", LARGE)
+def test_dos_moments_match_reference_build_at_size(name):
+    m = g.Model.load(fixture_dir(name))
+    H = g.Hamiltonian(m)
+    x = g.Vector.from_host(*m.initial_state())
+    rr, ri = ref_moments(name)
+    assert len(rr) == m.n_moments
+    fmts = [g.FORMAT_CODED, g.FORMAT_ELL] if H.format == g.FORMAT_CODED else [g.FORMAT_ELL]
+    got = []
+    for fmt in fmts:
+        H.set_format(fmt)
+        mr, mi = g.moments(H, x, x, m.n_moments)
+        assert _rel(mr, mi, rr, ri) <= REL_FP64, (name, fmt)
+        got.append((mr, mi))
+    if len(got) == 2:
+        # the two formats hold the same doubles: identical vectors, moments to the order
+        # of the FP64 sums
+        assert _rel(got[0][0], got[0][1], got[1][0], got[1][1]) <= REL_FP64
+
+
+@pytest.mark.gpu
+@pytest.mark.slow
+def test_msd_moments_match_reference_build_at_size():
+    """find_msd's moment sets on graphene 2M: evolve and evolvex of 1 fs (about 40
+    Bessel terms each) ahead of each 3000-moment set."""
+    name = "graphene2m"
+    m = g.Model.load(fixture_dir(name))
+    H = g.Hamiltonian(m)
+    ref = ref_npz(name, "msdmom")
+    steps, M = ref["re"].shape
+    phi = g.Vector.from_host(*m.initial_state())
+    ts = np.full(steps, m.time_step[0])
+    state, sx, copy = phi.clone(), phi.clone(), g.Vector(m.n)
+    g.evolve(H, 1, ts[0] * m.energy_max, state)
+    g.evolvex(H, 1, ts[0] * m.energy_max, sx)
+    for k in range(steps):
+        mr, mi = g.moments(H, sx, sx, M)
+        assert _rel(mr, mi, ref["re"][k], ref["im"][k]) <= REL_FP64, k
+        if k < steps - 1:
+            dt = ts[k + 1] * m.energy_max
+            copy.copy_from(state)
+            g.evolvex(H, 1, dt, copy)
+            g.evolve(H, 1, dt, sx)
+            sx.add(copy)
+            g.evolve(H, 1, dt, state)
