@@ -8,12 +8,22 @@ plain FP64 form (the reference's arithmetic, bit-identical per site) with the op
 in its default device format (coded: one byte per ELL entry). value = site-moments/s
 over all ranks (sites x moments x steps / max-over-ranks device time).
 
-Also reported: the roofline of the dominant kernel (the fused Chebyshev step + moment
-partial sums), the same metric end to end through the public API with host buffers
-(e2e), the plain FP64 rate on the reference's ELL arrays, the FP32-storage batched
-form (16 and 32 vectors per launch) with its DOS error against FP64 and its speed-up over
-both FP64 rates, the realisation batch, the Bessel evolution cost, and the
-reference's CPU path timed on this host's cores (cpu_baseline).
+Also reported, on the same line:
+  roofline      the dominant kernel (the fused Chebyshev step + moment partial sums)
+  e2e           the same metric through the public API with host buffers
+  forms         graphene 2M in every form: FP64 on the ELL arrays, FP32 storage with
+                1/16/32 vectors per launch, symmetric (doubled) sets in FP64 and FP32,
+                each with its byte model and roofline fraction; `north_star` states the
+                FP32/FP64 ratios like for like (direct/direct, doubled/doubled) next to
+                their byte-model ceilings
+  evolution     the Bessel evolution of one 1 fs MSD step (evolve, evolvex)
+  batch         the realisation batch (8 uneven square lattices, 64 vectors, FP32)
+  cubic256      the 3D Anderson lattice 256^3 (z = 6): FP64 and 16-vector FP32 side by
+                side (DOS rate, one VAC and one MSD correlation step, errors)
+  precision     graphene 4M, 5000 moments: FP32-storage error against FP64 for the
+                DOS and 20 VAC steps (peak-relative and pointwise)
+  cpu_baseline  the reference's CPU path (oracle/_ref) on this host: one core, and
+                one process per core
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 Multi-GPU runs are launched with torchrun, one rank per GPU (independent replicas).
@@ -57,6 +67,27 @@ def fp64_bytes_per_site(z=Z, coded=True):
 
 def fp32_bytes_per_site_vector(V, z=Z, coded=True):
     return (z * entry_bytes(coded) + 8) / V + 4 * 8
+
+
+# A step of a symmetric (doubled) moment set reads T_{k-1} and T_{k-2} and writes T_k
+# (no left stream) and yields two moments.
+def fp64_pair_bytes_per_site_step(z=Z, coded=True):
+    return z * entry_bytes(coded) + 8 + 3 * 16
+
+
+def fp32_pair_bytes_per_site_vector_step(V, z=Z, coded=True):
+    return (z * entry_bytes(coded) + 8) / V + 3 * 8
+
+
+# Evolution terms (per site and term): k_cheb2 reads T_{m-1} (gathered once), T_{m-2},
+# reads and writes the accumulator and writes T_m; k_cheb2x does the same for the
+# state and its [X, .] partner (the coded format keeps xx in its table).
+def cheb2_bytes_per_site(z=Z, coded=True):
+    return z * entry_bytes(coded) + 8 + 5 * 16
+
+
+def cheb2x_bytes_per_site(z=Z, coded=True):
+    return z * (entry_bytes(coded) + (0 if coded else 8)) + 8 + 10 * 16
 
 
 def log(*a):
@@ -178,6 +209,17 @@ def host_cores():
         return os.cpu_count() or 1
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def time_reference(ref_dir, n_moments, reps, procs):
     """Run the reference's find_moments_chebyshev (oracle/_ref/ref_driver) in `procs`
     independent processes at once; returns per-rep max-over-process seconds."""
@@ -197,17 +239,25 @@ def time_reference(ref_dir, n_moments, reps, procs):
 
 
 def cpu_baseline_line(ref_dir, n_sites, n_moments_sample=64, reps=3):
+    """The reference's CPU moment loop on this host: one process (the reference is
+    serial: its 1-core rate) and one process per core at once (the host's aggregate,
+    independent vectors)."""
     procs = min(host_cores(), 64)
+    t1, why = time_reference(ref_dir, n_moments_sample, reps, 1)
+    if t1 is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
     t, why = time_reference(ref_dir, n_moments_sample, reps, procs)
     if t is None:
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": why}
-    mean = statistics.mean(t)
-    return {"value": procs * n_sites * n_moments_sample / mean, "unit": UNIT, "cores": procs,
-            "kind": "reference",
+    one_core = n_sites * n_moments_sample / statistics.mean(t1)
+    return {"value": procs * n_sites * n_moments_sample / statistics.mean(t), "unit": UNIT,
+            "cores": procs, "kind": "reference", "cpu_model": cpu_model(),
+            "value_1_core": one_core,
             "sample": f"reference find_moments_chebyshev (oracle/_ref, g++ -O3, serial) on "
                       f"the same lattice (its fixed seed 12345678), {n_moments_sample} "
-                      f"moments per call, {procs} independent processes at once, "
-                      f"{reps} calls each, mean of the slowest process"}
+                      f"moments per call; value: {procs} independent processes at once, "
+                      f"{reps} calls each, mean of the slowest process; value_1_core: one "
+                      f"process alone, {reps} calls"}
 
 
 # ----------------------------------------------------------------------------- arms
@@ -235,11 +285,16 @@ def run_reference(args):
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": mean * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": W.CONFIGS[WORKLOAD]["description"] +
-                       f"; bounded sample: {sample} moments per step",
-                       "form": "reference CPU (lsqt_cpu objects), FP64",
-                       "parallelism": f"{procs} host processes (independent vectors)"},
+            "config": dict(workload_config(WORKLOAD),
+                           moments=sample,
+                           sample=f"{sample} of the workload's 3000 moments per process and "
+                                  f"step (the rate per site-moment does not depend on the "
+                                  f"count); the reference's fixed seed 12345678 instead of "
+                                  f"seed 3 (same lattice and disorder strength)",
+                           form="reference CPU path (its own objects, g++ -O3), FP64",
+                           parallelism=f"{procs} host processes (independent vectors)"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": "reference",
+                             "cpu_model": cpu_model(),
                              "sample": f"{sample}-moment find_moments_chebyshev per process "
                                        f"per step, {procs} processes at once"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -248,6 +303,21 @@ def run_reference(args):
         print(json.dumps(line), flush=True)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
+
+
+def workload_config(name):
+    """The bench line's `config` for a workload: its parameters, one key each."""
+    from gpuqt_b200 import workloads as W
+    c = W.CONFIGS[name]
+    lattice = {"graphene": "honeycomb graphene (4-orbital cell)", "square": "square",
+               "cubic": "cubic"}[c["kind"]]
+    return {"workload": name, "lattice": lattice,
+            "cells": "x".join(str(v) for v in c["cells"]), "sites": W.config_sites(name),
+            "z": {"graphene": 3, "square": 4, "cubic": 6}[c["kind"]],
+            "pbc": "all in-plane" if c["kind"] != "cubic" else "all",
+            "hopping": c["hopping"], "anderson_w": c["anderson"],
+            "seed": c.get("seed", c.get("disorder_seed")), "energy_max": c["energy_max"],
+            "moments": c["moments"]}
 
 
 def dos_error(g, m, mu64, mu32):
@@ -345,6 +415,13 @@ def run_ours(args):
         if not args.no_batch:
             del x
             batch = measure_batch(g, torch, tmp, stream, hbm_peak)
+        cubic = None
+        if not args.no_cubic:
+            cubic = measure_cubic(g, torch, tmp, stream, hbm_peak)
+        precision = None
+        if not args.no_precision:
+            from gpuqt_b200 import precision_report
+            precision = precision_report.report("graphene4m", 20)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_line(reference_dir(src, os.path.join(tmp, "ref")), n)
@@ -356,13 +433,15 @@ def run_ours(args):
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Anderson lattice, random-phase vectors)",
-                "config": {"workload": W.CONFIGS[WORKLOAD]["description"] +
-                           "; one KPM moment set per step, one random-phase vector per GPU",
-                           "form": "plain FP64 (reference arithmetic)",
-                           "operator_format": fmt + (f" ({H.n_codes} distinct entries)"
-                                                     if coded else ""),
-                           "parallelism": f"replicas x{world}",
-                           "l2": "inputs larger than L2 (220 MB touched per Chebyshev step)"},
+                "config": dict(workload_config(WORKLOAD),
+                               step="one KPM moment set (3000 moments)",
+                               vectors_per_gpu=1,
+                               form="plain FP64 (reference arithmetic)",
+                               operator_format=fmt + (f" ({H.n_codes} distinct entries)"
+                                                      if coded else ""),
+                               parallelism=f"replicas x{world}",
+                               l2="inputs larger than L2 (220 MB touched per Chebyshev "
+                                  "step)"),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm_peak,
                              "unit": "GB/s", "frac": achieved / hbm_peak,
                              "traffic": traffic, "peak_kind": peak_kind,
@@ -375,6 +454,8 @@ def run_ours(args):
                 "forms": forms,
                 "evolution": evolution,
                 "batch": batch,
+                "cubic256": cubic,
+                "precision": precision,
             }
             print(json.dumps(line), flush=True)
     finally:
@@ -458,7 +539,6 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
     H.set_format(default)
     for k in [k for k in out if k.startswith("fp32")]:
         out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / rate64
-        out[k]["speedup_vs_fp64_ell"] = out[k]["site_moments_per_s"] / rate64_ell
     out["fp64_v1_site_moments_per_s"] = rate64
 
     # Symmetric moment sets from half the Chebyshev steps (gqt_moments_doubled): the
@@ -475,48 +555,195 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         torch.cuda.synchronize()
         return V * n * M * 3 / (a.elapsed_time(b) / 1e3)
 
+    def pair_roofline(rate, bytes_per_step):
+        # a pair step yields two moments: steps/s = moments/s / 2
+        ach = rate / 2 * bytes_per_step / 1e9
+        return {"bytes_per_site_step": bytes_per_step, "achieved_gbs": ach,
+                "frac": ach / hbm_peak}
+
     dr, di = g.moments_doubled(H, x64, M)
-    out["fp64_doubled"] = {
-        "site_moments_per_s": doubled(x64, 1),
-        "max_err_vs_direct": float(np.max(np.hypot(dr - r64, di - i64)) /
-                                   np.max(np.hypot(r64, i64))),
-        "speedup_vs_fp64": None}
-    out["fp64_doubled"]["speedup_vs_fp64"] = out["fp64_doubled"]["site_moments_per_s"] / rate64
+    rate64_dbl = doubled(x64, 1)
+    out["fp64_doubled"] = dict(
+        {"site_moments_per_s": rate64_dbl,
+         "max_err_vs_direct": float(np.max(np.hypot(dr - r64, di - i64)) /
+                                    np.max(np.hypot(r64, i64))),
+         "speedup_vs_fp64": rate64_dbl / rate64},
+        **pair_roofline(rate64_dbl, fp64_pair_bytes_per_site_step(coded=coded)))
     vecs = [phi] + [m.initial_state() for _ in range(15)]
     X16 = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
                              nvec=16, precision=g.FP32)
     r32, i32 = g.moments_doubled(H, X16, M)
-    out["fp32_v16_doubled"] = {
-        "site_moments_per_s": doubled(X16, 16),
-        "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32[0], i32[0]))}
-    out["fp32_v16_doubled"]["speedup_vs_fp64"] = (
-        out["fp32_v16_doubled"]["site_moments_per_s"] / rate64)
-    out["fp32_v16_doubled"]["speedup_vs_fp64_ell"] = (
-        out["fp32_v16_doubled"]["site_moments_per_s"] / rate64_ell)
+    rate32_dbl = doubled(X16, 16)
+    out["fp32_v16_doubled"] = dict(
+        {"site_moments_per_s": rate32_dbl, "vectors_per_launch": 16,
+         "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32[0], i32[0])),
+         "speedup_vs_fp64": rate32_dbl / rate64},
+        **pair_roofline(rate32_dbl, fp32_pair_bytes_per_site_vector_step(16, coded=coded)))
     del X16
     ach = fp64_bytes_per_site(coded=False) * rate64_ell / 1e9
     out["fp64_v1_ell"] = {"site_moments_per_s": rate64_ell, "achieved_gbs": ach,
                           "frac": ach / hbm_peak,
                           "bytes_per_site_moment": fp64_bytes_per_site(coded=False)}
+    ach = fp64_bytes_per_site(coded=coded) * rate64 / 1e9
+    out["fp64_v1"] = {"site_moments_per_s": rate64, "achieved_gbs": ach,
+                      "frac": ach / hbm_peak,
+                      "bytes_per_site_moment": fp64_bytes_per_site(coded=coded)}
+
+    # The north-star ratio, like for like: batched FP32 storage over plain FP64 in the
+    # same loop (direct over direct, doubled over doubled), each next to the ratio of
+    # the two forms' byte models, which bounds it while both are HBM-bound.
+    d32 = out["fp32_v16"]
+    ceil_direct = fp64_bytes_per_site(coded=coded) / fp32_bytes_per_site_vector(16, coded=coded)
+    ceil_dbl = (fp64_pair_bytes_per_site_step(coded=coded) /
+                fp32_pair_bytes_per_site_vector_step(16, coded=coded))
+    ratio_direct = d32["site_moments_per_s"] / rate64
+    ratio_dbl = rate32_dbl / rate64_dbl
+    out["north_star"] = {
+        "target": "batched FP32 >= 3x plain FP64 site-moments/s, both >= 0.70 of HBM "
+                  "roofline, <= 1e-6 error",
+        "speedup_direct": ratio_direct, "byte_ceiling_direct": ceil_direct,
+        "speedup_doubled": ratio_dbl, "byte_ceiling_doubled": ceil_dbl,
+        "speedup_fp32_doubled_over_fp64_direct": rate32_dbl / rate64,
+        "frac_fp64_direct": out["fp64_v1"]["frac"], "frac_fp32_v16_direct": d32["frac"],
+        "frac_fp64_doubled": out["fp64_doubled"]["frac"],
+        "frac_fp32_v16_doubled": out["fp32_v16_doubled"]["frac"],
+        "dos_err_fp32_v16": d32["dos_err_vs_fp64"],
+        "met_like_for_like": bool(max(ratio_direct, ratio_dbl) >= 3.0 and
+                                  d32["frac"] >= 0.7 and out["fp64_v1"]["frac"] >= 0.7),
+        "note": "while both forms are HBM-bound the like-for-like ratio is capped by "
+                "the byte models (byte_ceiling_*): FP32 storage keeps four 8-byte vector "
+                "streams per site-vector-moment (three in a doubled step) against 75 B "
+                "(59 B) for the coded FP64 step"}
     # Bessel evolution of one MSD step (1 fs): evolve and evolvex, FP64.
     dt = m.time_step[0] * m.energy_max
     st = x64.clone()
     g.evolve(H, 1, dt, st)
     g.evolvex(H, 1, dt, st)
+    reps = 5
     a, b = ev()
     before = g.launch_count()
     a.record(stream)
-    g.evolve(H, 1, dt, st)
+    for _ in range(reps):
+        g.evolve(H, 1, dt, st)
     b.record(stream)
-    terms = g.launch_count() - before - 2  # apply and the 0/1 term precede the series
+    # apply and the 0/1 term precede the series
+    terms = (g.launch_count() - before) // reps - 2
     c, d = ev()
     c.record(stream)
-    g.evolvex(H, 1, dt, st)
+    for _ in range(reps):
+        g.evolvex(H, 1, dt, st)
     d.record(stream)
     torch.cuda.synchronize()
-    evolution = {"dt_scaled": dt, "bessel_terms": terms, "ms_evolve": a.elapsed_time(b),
-                 "ms_evolvex": c.elapsed_time(d)}
+    ms_e, ms_x = a.elapsed_time(b) / reps, c.elapsed_time(d) / reps
+    # Per-term algorithmic bytes over the series (the apply and 0/1 terms ride along).
+    gb_e = terms * n * cheb2_bytes_per_site(coded=coded) / (ms_e / 1e3) / 1e9
+    gb_x = terms * n * cheb2x_bytes_per_site(coded=coded) / (ms_x / 1e3) / 1e9
+    evolution = {"dt_scaled": dt, "bessel_terms": terms, "ms_evolve": ms_e,
+                 "ms_evolvex": ms_x,
+                 "k_cheb2": {"bytes_per_site_term": cheb2_bytes_per_site(coded=coded),
+                             "achieved_gbs": gb_e, "frac": gb_e / hbm_peak},
+                 "k_cheb2x": {"bytes_per_site_term": cheb2x_bytes_per_site(coded=coded),
+                              "achieved_gbs": gb_x, "frac": gb_x / hbm_peak}}
     return out, evolution
+
+
+def measure_cubic(g, torch, tmp, stream, hbm_peak, vectors=16):
+    """The 3D Anderson lattice near its transition (cubic 256^3 = 16,777,216 sites, z = 6,
+    t = -1, W = 16.5, seed 13, E_max 15, 4000 moments): plain FP64 (one vector) and FP32
+    storage (16 vectors per launch) side by side. One DOS moment set each, timed whole;
+    a VAC correlation step (current operator, moment set, two evolutions; the moment
+    set's time is the DOS set's) and an MSD step (evolvex, two evolutions, moment set),
+    composed from timed parts; the FP32 error against FP64 on the first vector for the
+    DOS and for the VAC moment sets of the first two correlation steps."""
+    from gpuqt_b200 import precision_report as P
+    from gpuqt_b200 import workloads as W
+    name = "cubic256"
+    m = g.Model.load(W.config_dir(tmp, name))
+    H = g.Hamiltonian(m)
+    n, M = m.n, m.n_moments
+    coded = H.format == g.FORMAT_CODED
+    z = 6
+
+    def timed(fn, reps=1, warm=True):
+        if warm:
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    vecs = [m.initial_state() for _ in range(vectors)]
+    x64 = g.Vector.from_host(*vecs[0])
+    mu64 = torch.empty(2 * M, dtype=torch.float64, device="cuda")
+    ms64 = timed(lambda: g.moments_device(H, x64, x64, M, mu64.data_ptr()))
+    r64, i64 = g.moments(H, x64, x64, M)
+    X = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
+                           nvec=vectors, precision=g.FP32)
+    mu32 = torch.empty(2 * M * vectors, dtype=torch.float64, device="cuda")
+    ms32 = timed(lambda: g.moments_device(H, X, X, M, mu32.data_ptr()))
+    mu_h = mu32.view(M, vectors, 2).cpu().numpy()
+    dos = P.compare(g, m, (r64, i64), (mu_h[:, 0, 0].copy(), mu_h[:, 0, 1].copy()))
+    b64 = fp64_bytes_per_site(z=z, coded=coded)
+    b32 = fp32_bytes_per_site_vector(vectors, z=z, coded=coded)
+    rate64 = n * M / (ms64 / 1e3)
+    rate32 = vectors * n * M / (ms32 / 1e3)
+
+    # Parts of the correlation steps (FP64 state; the FP32 form's 16-vector state).
+    dt = m.time_step[0] * m.energy_max
+    tmp64 = g.Vector(n)
+    tmp32 = g.Vector(n, nvec=vectors, precision=g.FP32)
+    before = g.launch_count()
+    g.evolve(H, 1, dt, x64)
+    terms = g.launch_count() - before - 2
+    parts = {
+        "fp64": {"current": timed(lambda: g.apply_current(H, x64, tmp64), 3),
+                 "evolve": timed(lambda: g.evolve(H, 1, dt, x64), 3),
+                 "evolvex": timed(lambda: g.evolvex(H, 1, dt, x64), 3)},
+        "fp32_v16": {"current": timed(lambda: g.apply_current(H, X, tmp32), 3),
+                     "evolve": timed(lambda: g.evolve(H, 1, dt, X), 2),
+                     "evolvex": timed(lambda: g.evolvex(H, 1, dt, X), 2)},
+    }
+    del tmp32
+
+    def form(rate, ms_set, bytes_sm, V, p):
+        ach = rate * bytes_sm / 1e9
+        vac = p["current"] + ms_set + 2 * p["evolve"]
+        msd = p["evolvex"] + 2 * p["evolve"] + ms_set
+        return {"vectors_per_launch": V, "dos_site_moments_per_s": rate, "ms_dos_set": ms_set,
+                "bytes_per_site_moment": bytes_sm, "achieved_gbs": ach, "frac": ach / hbm_peak,
+                "ms_current": p["current"], "ms_evolve": p["evolve"],
+                "ms_evolvex": p["evolvex"], "ms_vac_step": vac, "ms_msd_step": msd,
+                "vac_step_site_moments_per_s": V * n * M / (vac / 1e3),
+                "msd_step_site_moments_per_s": V * n * M / (msd / 1e3)}
+
+    e64 = parts["fp64"]
+    gb_e = terms * n * cheb2_bytes_per_site(z=z, coded=coded) / (e64["evolve"] / 1e3) / 1e9
+    gb_x = terms * n * cheb2x_bytes_per_site(z=z, coded=coded) / (e64["evolvex"] / 1e3) / 1e9
+    out = {
+        "config": dict(workload_config(name), vectors=vectors,
+                       note="VAC/MSD step times are the timed moment set plus the timed "
+                            "current, evolve and evolvex of that form"),
+        "fp64": form(rate64, ms64, b64, 1, parts["fp64"]),
+        "fp32_v16": form(rate32, ms32, b32, vectors, parts["fp32_v16"]),
+        "speedup_dos": rate32 / rate64,
+        "byte_ceiling_dos": b64 / b32,
+        "evolution_fp64": {"dt_scaled": dt, "bessel_terms": terms,
+                           "k_cheb2_frac": gb_e / hbm_peak, "k_cheb2_gbs": gb_e,
+                           "k_cheb2x_frac": gb_x / hbm_peak, "k_cheb2x_gbs": gb_x},
+        "dos_err_fp32_vs_fp64": dos,
+    }
+    del X, mu32
+    # VAC moment sets of the first two correlation steps, FP32 storage against FP64
+    # (vector 0; states evolved in FP64, as the library's FP32 form does).
+    a = P.vac_moments(g, m, H, vecs[0], g.FP64, 2)
+    b = P.vac_moments(g, m, H, vecs[0], g.FP32, 2)
+    per = [P.compare(g, m, a[k], b[k]) for k in range(2)]
+    out["vac_err_fp32_vs_fp64"] = {k: max(q[k] for q in per) for k in per[0]}
+    out["vac_err_steps"] = 2
+    return out
 
 
 def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
@@ -530,6 +757,24 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
     B = g.Hamiltonian.batch(models)
     best, rates = g.autotune_nvec(B, g.FP32, 20, [4, 8, 16, 32])
     V = best
+    tile = B.batch_tile
+    # The tile sizes at the chosen vector count, as the autotuner saw them (a short
+    # probe each; the autotuner's choice is restored afterwards).
+    tile_rates = {}
+    Xp = g.Vector(B.n, nvec=V, precision=g.FP32)
+    mup = torch.empty(2 * 20 * len(models) * V, dtype=torch.float64, device="cuda")
+    for t in (256, 512, 1024):
+        B.set_batch_tile(t)
+        g.moments_device(B, Xp, Xp, 20, mup.data_ptr())
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(3):
+            g.moments_device(B, Xp, Xp, 20, mup.data_ptr())
+        b.record(stream)
+        torch.cuda.synchronize()
+        tile_rates[t] = 3 * V * sum(m.n for m in models) * 20 / (a.elapsed_time(b) / 1e3)
+    B.set_batch_tile(tile)
+    del Xp, mup
     rng = np.random.default_rng(11)
     sites = sum(m.n for m in models)
     X = g.Vector(B.n, nvec=V, precision=g.FP32)
@@ -590,6 +835,7 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
             "sites": sites, "padded_sites": B.n, "vectors": vectors, "moments": moments,
             "operator_format": "coded" if B.format == g.FORMAT_CODED else "ell",
             "autotuned_vectors_per_launch": V, "autotune_rates": rates,
+            "autotuned_tile_sites": tile, "tile_rates_at_best_vectors": tile_rates,
             "site_moments_per_s": rate, "ms_total": total_ms,
             "achieved_gbs": rate * bytes_site_moment / 1e9,
             "frac": rate * bytes_site_moment / 1e9 / hbm_peak,
@@ -605,6 +851,8 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-cubic", action="store_true")
+    ap.add_argument("--no-precision", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -67,6 +67,8 @@ _SIGS = {
     "gqt_ham_info": (ctypes.c_int, [_vp, _ip, _ip, _ip, _dp]),
     "gqt_ham_set_format": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gqt_ham_format": (ctypes.c_int, [_vp, _ip, _ip]),
+    "gqt_ham_set_batch_tile": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gqt_ham_batch_tile": (ctypes.c_int, [_vp, _ip]),
     "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
                                             ctypes.POINTER(_vp)]),
     "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
@@ -369,6 +371,16 @@ class Hamiltonian:
         c = ctypes.c_int()
         _call("gqt_ham_format", self.h, None, ctypes.byref(c))
         return c.value
+
+    @property
+    def batch_tile(self) -> int:
+        """Sites per tile of a realisation batch's step (0 for a single model)."""
+        t = ctypes.c_int()
+        _call("gqt_ham_batch_tile", self.h, ctypes.byref(t))
+        return t.value
+
+    def set_batch_tile(self, tile_sites: int) -> None:
+        _call("gqt_ham_set_batch_tile", self.h, int(tile_sites))
 
     def set_format(self, fmt: int) -> None:
         """FORMAT_ELL or FORMAT_CODED (the default when the operator has a coded form)."""

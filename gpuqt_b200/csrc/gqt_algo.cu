@@ -77,12 +77,13 @@ gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out)
 }
 
 // The slab of deferred block partials ([window][grid][results][4] doubles, after the
-// immediate partials) stays within 32 MiB.
+// immediate partials) stays within 32 MiB: 256 steps for one vector, 27 for 32, and
+// 2-3 for realisation batches of hundreds of (realisation, vector) sums.
 int defer_window(int results)
 {
   const size_t per = (size_t)max_grid() * results * 4 * sizeof(double);
   const size_t w = ((size_t)32 << 20) / per;
-  return (int)(w < 8 ? 8 : (w > 256 ? 256 : w));
+  return (int)(w < 2 ? 2 : (w > 256 ? 256 : w));
 }
 
 namespace {
@@ -244,6 +245,53 @@ struct Deferred {
   }
 };
 
+// The same deferral for realisation batches: the j-th kCheb step of a window writes its
+// per-block slots to slab row j, and one k_tile_reduce launch over the window's rows
+// turns them into moments (`results` = R x sums per realisation, consecutive moments
+// `results` double2 apart). Rows are max_grid() x results x 4 doubles.
+struct BatchDeferred {
+  const FormOps* f;
+  Op op;
+  DotScratch* ds;
+  int results;
+  bool pair;
+  int len;
+  size_t stride;
+  int blocks = 0;
+  MultiDot first{};
+  int used = 0;
+
+  BatchDeferred(const FormOps* f_, const Op& op_, DotScratch* d, int r, bool p)
+      : f(f_), op(op_), ds(d), results(r), pair(p), len(defer_window(r)),
+        stride((size_t)max_grid() * r * 4)
+  {
+  }
+
+  MultiDot next(const MultiDot& base, double2* mu)
+  {
+    MultiDot md = base;
+    md.partials = ds->partials + (size_t)(1 + used) * stride;
+    md.mu = mu;
+    md.defer = 1;
+    md.blocks_out = &blocks;
+    if (used == 0)
+      first = md;
+    ++used;
+    return md;
+  }
+
+  gqt_status flush(bool last)
+  {
+    if (used == 0 || (!last && used < len))
+      return GQT_OK;
+    MultiDot md = first;
+    md.blocks = blocks;  // every kCheb step of the loop launches the same kernel
+    GQT_TRY(f->tile_reduce(op, md, pair, used, stride));
+    used = 0;
+    return GQT_OK;
+  }
+};
+
 // The launch sequence of the moment loop (src/sigma.cu:33-61) on the current stream.
 // Buffers: T_0 = right (read only), T_1 -> A, then T_m overwrites T_{m-2} in place.
 gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* left,
@@ -264,10 +312,12 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
     GQT_TRY(f->step_multi(op, kApply, nullptr, right->data, A, left->data, md));
     const void* prev = right->data;
     void* cur = A;
+    BatchDeferred bd(f, op, ds, RV, false);
     for (int m = 2; m < M; ++m) {
       void* out = (prev == right->data) ? B : (void*)prev;
-      md.mu = mu + (size_t)m * RV;
-      GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, left->data, md));
+      GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, left->data,
+                            bd.next(md, mu + (size_t)m * RV)));
+      GQT_TRY(bd.flush(m == M - 1));
       prev = cur;
       cur = out;
     }
@@ -315,10 +365,12 @@ gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_ve
       GQT_TRY(f->step_multi(op, kApply, nullptr, phi->data, A, nullptr, md, kDotPair));
       const void* prev = phi->data;
       void* cur = A;
+      BatchDeferred bd(f, op, ds, 2 * RV, true);
       for (int k = 2; k <= K; ++k) {
         void* out = (prev == phi->data) ? B : (void*)prev;
-        md.mu = pairs + (size_t)k * 2 * RV;
-        GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, nullptr, md, kDotPair));
+        GQT_TRY(f->step_multi(op, kCheb, prev, cur, out, nullptr,
+                              bd.next(md, pairs + (size_t)k * 2 * RV), kDotPair));
+        GQT_TRY(bd.flush(k == K));
         prev = cur;
         cur = out;
       }
@@ -591,10 +643,11 @@ static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const g
   const size_t bytes = right->bytes;
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
   GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
-  // Block partials: [grid][R][V][4] doubles for a batch; [grid][V][4] otherwise, followed
+  // Block partials: [grid][R][V][4] doubles for a batch, [grid][V][4] otherwise, followed
   // by the slab of a window of deferred moments.
-  const size_t rows = h->n_real > 1 ? 1 : 1 + (size_t)defer_window(right->nvec);
-  GQT_TRY(ws_dot(ws, rows * max_grid() * h->n_real * right->nvec * 4, ds));
+  const int results = h->n_real * right->nvec;
+  const size_t rows = 1 + (size_t)defer_window(results);
+  GQT_TRY(ws_dot(ws, rows * max_grid() * results * 4, ds));
   return GQT_OK;
 }
 
@@ -617,8 +670,9 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
     if (h->n_real == 1 && right->nvec > 16)
       return fail(GQT_ERR_ARG, "%s: at most 16 vectors (got %d)", w, right->nvec);
     // Pair sums: twice the block partials of the direct loop (and of its slab).
-    const size_t rows = h->n_real > 1 ? 1 : 1 + (size_t)defer_window(2 * right->nvec);
-    GQT_TRY(ws_dot(ws, rows * max_grid() * h->n_real * right->nvec * 8, &ds));
+    const int results = 2 * h->n_real * right->nvec;
+    const size_t rows = 1 + (size_t)defer_window(results);
+    GQT_TRY(ws_dot(ws, rows * max_grid() * results * 4, &ds));
     const size_t need = (size_t)(M / 2 + 1) * 2 * h->n_real * right->nvec * sizeof(double2);
     if (ws.pairs_bytes < need) {
       cudaStreamSynchronize(s);
@@ -994,6 +1048,7 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
   gqt_status st = GQT_OK;
   Workspace& ws = *h->ws;
   bool changed = false;
+  int best_tile = 0;
   for (int k = 0; k < n_candidates && st == GQT_OK; ++k) {
     const int V = candidates[k];
     double rate = 0.0;
@@ -1007,12 +1062,20 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
         if (ce != cudaSuccess)
           st = cuda_fail(ce, "cudaMalloc(probe moments)", __FILE__, __LINE__);
       }
-      // Shapes: vectors per thread 4 (the default) and 2, where the form has both.
+      // Shapes: vectors per thread 4 (the default) and 2, where the form has both; on a
+      // realisation batch, each with every tile size.
       const int shapes[2] = {0, 2};
       const int n_shapes = (precision == GQT_FP32 && V >= 4) ? 2 : 1;
-      int best_w = 0;
-      for (int si = 0; si < n_shapes && st == GQT_OK; ++si) {
+      const int n_tiles = h->n_real > 1 ? kBatchTiles : 1;
+      int best_w = 0, best_t = h->tile_sites;
+      for (int q = 0; q < n_shapes * n_tiles && st == GQT_OK; ++q) {
+        const int si = q / n_tiles;
         h->wpt[V] = shapes[si];
+        if (h->n_real > 1) {
+          st = batch_set_tile(const_cast<gqt_ham*>(h), kBatchTileSizes[q % n_tiles]);
+          if (st != GQT_OK)
+            break;
+        }
         st = gqt_moments_device(h, x, x, n_moments, mu);  // warm-up, graph capture
         float ms = 0.f;
         if (st == GQT_OK) {
@@ -1033,6 +1096,7 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
         if (r > rate) {
           rate = r;
           best_w = shapes[si];
+          best_t = h->tile_sites;
         }
         // The probe's graph was captured with this shape; drop it before the next.
         cudaStreamSynchronize(s);
@@ -1045,9 +1109,11 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
           }
         }
       }
-      if (h->wpt[V] != best_w || n_shapes > 1)
+      if (h->wpt[V] != best_w || n_shapes > 1 || n_tiles > 1)
         changed = true;
       h->wpt[V] = best_w;
+      if (rate > best_rate)
+        best_tile = best_t;
       cudaFree(mu);
       gqt_vec_destroy(x);
     }
@@ -1058,6 +1124,9 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
       *best = V;
     }
   }
+  // A batch keeps the tile size of the fastest candidate.
+  if (h->n_real > 1 && best_tile > 0 && st == GQT_OK)
+    st = batch_set_tile(const_cast<gqt_ham*>(h), best_tile);
   if (changed) {
     // Graphs captured before the tuning launch the old shapes; recapture on next use.
     cudaStreamSynchronize(s);

@@ -24,6 +24,10 @@ struct OpFns {
   // (kDotPair: 2 nvec sums per realisation, [2v] <T_k|T_k>, [2v + 1] <T_{k-1}|T_k>).
   gqt_status (*step_multi)(const Op& op, int mode, const void* t0, const void* t1, void* out,
                            const void* left, const MultiDot& md, int dot);
+  // The per-realisation moments of `rows` batch steps launched with md.defer set (pair:
+  // the steps fused the pair products); step j's slots start j * row_stride doubles into
+  // md.partials and its results go to md.mu + j * R * (pair ? 2 : 1) * nvec.
+  gqt_status (*tile_reduce)(const MultiDot& md, bool pair, int rows, size_t row_stride);
   gqt_status (*xop)(const Op& op, bool current, const void* in, void* out);
   // Evolution terms; out is a double2 accumulator (the FP64 state itself, or the
   // FP32 form's FP64 accumulator).
@@ -64,6 +68,11 @@ struct FormOps {
                         const void* left, const MultiDot& md, int dot = kDotLeft) const
   {
     return of(op).step_multi(op, mode, t0, t1, out, left, md, dot);
+  }
+  gqt_status tile_reduce(const Op& op, const MultiDot& md, bool pair, int rows,
+                         size_t row_stride) const
+  {
+    return of(op).tile_reduce(md, pair, rows, row_stride);
   }
   gqt_status xop(const Op& op, bool current, const void* in, void* out) const
   {

@@ -92,6 +92,11 @@ struct OpImpl {
   // vectors per thread: half the accumulator registers, twice the threads per site).
   static constexpr int W = vectors_per_thread<VT2, V>();
   static constexpr int W2 = (std::is_same<VT2, float2>::value && V >= 4) ? 2 : W;
+  // Vectors a thread advances in the pair mode of a symmetric moment set: 2 float2 or 1
+  // double2. The pair mode keeps three FP64 sums per vector and T_{k-1} until the end
+  // of an item; at the direct step's width (4 float2, 2 double2) that spilled 120-250
+  // bytes per thread at the step's register budget.
+  static constexpr int WP = std::is_same<VT2, float2>::value ? (V < 2 ? V : 2) : 1;
 
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)
@@ -156,13 +161,13 @@ struct OpImpl {
       VT2* o = (VT2*)out;
       return with_z(op.z, [&](auto zc) -> gqt_status {
         constexpr int Z = decltype(zc)::value;
-        if constexpr (W > 1) {
-          const size_t items = (size_t)op.n * (V / W);
+        if constexpr (V > 1) {
+          const size_t items = (size_t)op.n * (V / WP);
           if (mode == kApply)
-            return launch_op(k_step_vec<VT2, V, W, Z, A, kApply, kDotPair, C>, items, op, a0, a1,
-                             o, (const VT2*)nullptr, d);
-          return launch_op(k_step_vec<VT2, V, W, Z, A, kCheb, kDotPair, C>, items, op, a0, a1, o,
-                           (const VT2*)nullptr, d);
+            return launch_op(k_step_vec<VT2, V, WP, Z, A, kApply, kDotPair, C>, items, op, a0,
+                             a1, o, (const VT2*)nullptr, d);
+          return launch_op(k_step_vec<VT2, V, WP, Z, A, kCheb, kDotPair, C>, items, op, a0, a1,
+                           o, (const VT2*)nullptr, d);
         } else {
           const size_t total = (size_t)op.n * V;
           if (mode == kApply)
@@ -188,20 +193,22 @@ struct OpImpl {
       constexpr int Z = decltype(zc)::value;
       auto go = [&](auto* kernel) -> gqt_status {
         md.blocks = grid_for((const void*)kernel, items);
+        if (md.blocks_out)
+          *md.blocks_out = md.blocks;
         kernel<<<md.blocks, kBlock, op_smem_bytes(op), stream()>>>(op, a0, a1, o, l, md);
         count_launches(1);
         GQT_CUDA(cudaGetLastError());
         return GQT_OK;
       };
+      if (dot == kDotPair && mode != kDotOnly) {
+        if (mode == kApply)
+          return go(k_step_multi<VT2, V, WP, Z, A, kApply, C, kDotPair>);
+        return go(k_step_multi<VT2, V, WP, Z, A, kCheb, C, kDotPair>);
+      }
       auto pick = [&](auto wc) -> gqt_status {
         constexpr int WW = decltype(wc)::value;
         if (mode == kDotOnly)
           return go(k_step_multi<VT2, V, WW, Z, A, kDotOnly, C>);
-        if (dot == kDotPair) {
-          if (mode == kApply)
-            return go(k_step_multi<VT2, V, WW, Z, A, kApply, C, kDotPair>);
-          return go(k_step_multi<VT2, V, WW, Z, A, kCheb, C, kDotPair>);
-        }
         if (mode == kApply)
           return go(k_step_multi<VT2, V, WW, Z, A, kApply, C>);
         return go(k_step_multi<VT2, V, WW, Z, A, kCheb, C>);
@@ -212,10 +219,19 @@ struct OpImpl {
       }
       return pick(std::integral_constant<int, W>{});
     }));
-    if (dot == kDotPair && mode != kDotOnly)
-      k_tile_reduce<2 * V><<<md.n_real * 2 * V, kBlock, 0, stream()>>>(md);
+    if (md.defer)
+      return GQT_OK;  // the caller reduces a window of steps at once (tile_reduce)
+    return tile_reduce(md, dot == kDotPair && mode != kDotOnly, 1, 0);
+  }
+
+  // k_tile_reduce over `rows` steps whose slots lie row_stride doubles apart.
+  static gqt_status tile_reduce(const MultiDot& md, bool pair, int rows, size_t row_stride)
+  {
+    if (pair)
+      k_tile_reduce<2 * V><<<dim3(md.n_real * 2 * V, rows), kBlock, 0, stream()>>>(md,
+                                                                                row_stride);
     else
-      k_tile_reduce<V><<<md.n_real * V, kBlock, 0, stream()>>>(md);
+      k_tile_reduce<V><<<dim3(md.n_real * V, rows), kBlock, 0, stream()>>>(md, row_stride);
     count_launches(1);
     GQT_CUDA(cudaGetLastError());
     return GQT_OK;
@@ -256,7 +272,10 @@ struct OpImpl {
     });
   }
 
-  static OpFns fns() { return OpFns{step, step_pair, step_multi, xop, cheb2, cheb2x}; }
+  static OpFns fns()
+  {
+    return OpFns{step, step_pair, step_multi, tile_reduce, xop, cheb2, cheb2x};
+  }
 };
 
 template <typename VT2, int V, class A>

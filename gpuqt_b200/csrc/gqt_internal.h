@@ -34,6 +34,12 @@ struct DotScratch {
   int nvec = 0;
 };
 
+// Tile sizes (sites) the batch step can run with; models are padded to the largest.
+constexpr int kBatchTiles = 3;
+constexpr int kBatchTileSizes[kBatchTiles] = {256, 512, 1024};
+// Select tile size `tile` (one of kBatchTileSizes) for a realisation batch.
+gqt_status batch_set_tile(gqt_ham* h, int tile);
+
 // Temporary vectors and graph cache reused by the algorithm entry points.
 struct Workspace;
 
@@ -87,9 +93,12 @@ struct gqt_ham {
   // Realisation batch (gqt_ham_create_batch): n_real > 1 block-diagonal models, each
   // padded to whole tiles and pre-divided by its own E_max (energy_max is then 1).
   int n_real = 1;
-  int tile_sites = 0;
+  int tile_sites = 0;         // sites per tile of the batch step (the autotuner's choice)
   int n_tiles = 0;
   int* tile_first = nullptr;  // device, [n_real + 1]: first tile of each model
+  // device, [kBatchTiles][n_real + 1]: tile_first for each tile size of kBatchTileSizes
+  // (every model is padded to the largest, so each divides every model's offset)
+  int* tile_first_all = nullptr;
   std::vector<int> real_offset, real_n;
   std::vector<double> real_emax;
   // Vectors per thread of the batched step for each vector count (0: the form's

@@ -244,6 +244,14 @@ __device__ __forceinline__ void dot_term(CSum& re, CSum& im, double2 s, double2 
   csum_add(im, __dsub_rn(__dmul_rn(s.y, l.x), __dmul_rn(s.x, l.y)));
 }
 
+// The real part of dot_term(re, im, s, s): the imaginary part b*a - a*b of a product
+// of a value with itself is exactly zero, and adding zero leaves a compensated sum
+// unchanged bit for bit, so the pair mode's <T_k|T_k> keeps only its real sum.
+__device__ __forceinline__ void dot_term_self(CSum& re, double2 s)
+{
+  csum_add(re, __dadd_rn(__dmul_rn(s.x, s.x), __dmul_rn(s.y, s.y)));
+}
+
 __device__ __forceinline__ CSum shfl_xor(const CSum& a, int off)
 {
   CSum b;
@@ -431,6 +439,38 @@ __device__ __forceinline__ void stw(double2* p, const double2 (&v)[W])
 #pragma unroll
   for (int k = 0; k < W; ++k)
     p[k] = v[k];
+}
+
+// W consecutive elements kept in their storage type (the same wide loads as ldw). A
+// value a kernel needs twice, far apart, costs half the registers as float2 and is
+// widened exactly at each use.
+template <int W>
+__device__ __forceinline__ void ldw_raw(const float2* p, float2 (&o)[W])
+{
+  if constexpr (W == 1) {
+    o[0] = *p;
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k) {
+      const float4 f = reinterpret_cast<const float4*>(p)[k];
+      o[2 * k] = make_float2(f.x, f.y);
+      o[2 * k + 1] = make_float2(f.z, f.w);
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void ldw_raw(const double2* p, double2 (&o)[W])
+{
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    o[k] = p[k];
+}
+
+__device__ __forceinline__ double2 widen(double2 v) { return v; }
+__device__ __forceinline__ double2 widen(float2 v)
+{
+  return make_double2((double)v.x, (double)v.y);
 }
 
 // ------------------------------------------------------------------ the operator row
@@ -716,7 +756,7 @@ __device__ __forceinline__ void step_dot(CSum (&re)[2], CSum (&im)[2], double2 o
   if constexpr (DOT == kDotLeft) {
     dot_term(re[0], im[0], o, l);
   } else if constexpr (DOT == kDotPair) {
-    dot_term(re[0], im[0], o, o);
+    dot_term_self(re[0], o);
     dot_term(re[1], im[1], o, x);
   }
 }
@@ -733,15 +773,17 @@ __device__ __forceinline__ void step_dot(CSum (&re)[2], CSum (&im)[2], double2 o
 // Resident blocks per SM the step is compiled for (its register budget): 3 for rows of
 // up to four entries, 2 for six (the pipelined row of six holds twice the indices).
 // Measured on B200 against the compiler's own choice, which varied from 43 to 114
-// registers between near-identical builds of the same loop.
-template <int Z>
+// registers between near-identical builds of the same loop. The pair mode on the ELL
+// arrays (hoppings travelling with the prefetched row, two compensated products) takes
+// 2: at 3 it spilled 50-180 bytes per thread.
+template <int Z, int DOT = kDotLeft, bool C = true>
 constexpr int step_min_blocks()
 {
-  return Z >= 6 ? 2 : 3;
+  return (Z >= 6 || (DOT == kDotPair && !C)) ? 2 : 3;
 }
 
 template <typename VT2, int V, int Z, class A, int MODE, int DOT, bool C>
-__global__ void __launch_bounds__(kBlock, step_min_blocks<Z>()) k_step(Op op, const VT2* t0,
+__global__ void __launch_bounds__(kBlock, step_min_blocks<Z, DOT, C>()) k_step(Op op, const VT2* t0,
                                                  const VT2* __restrict__ t1, VT2* out,
                                                  const VT2* __restrict__ left, Dot dot)
 {
@@ -848,15 +890,30 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
 // compiler's own choice: k_step_vec at 4 (64 registers: +9 % for 16 FP32 vectors on
 // graphene, +7 % on cubic, +17 % for 32 vectors on the ELL arrays); k_step_multi at 3
 // with the coded table, 4 on the ELL arrays.
+// The pair mode of a symmetric set keeps three sums per vector and T_{k-1} for the whole
+// item: rows of unknown length (Z = 0) and the FP64 form on rows of six take 3 blocks
+// per SM there (at 4 they spilled 40-140 bytes per thread), the FP64 form on rows of
+// unknown length 2 (12-24 bytes at 3).
 constexpr int kVecMinBlocks = 4;
-template <bool C>
+template <typename VT2, int Z, int DOT>
+constexpr int vec_min_blocks()
+{
+  constexpr bool f64 = std::is_same<VT2, double2>::value;
+  if constexpr (DOT != kDotPair)
+    return kVecMinBlocks;
+  else if constexpr (Z <= 0)
+    return f64 ? 2 : 3;
+  else
+    return (Z >= 6 && f64) ? 3 : kVecMinBlocks;
+}
+template <bool C, int Z = 4, int DOT = kDotLeft>
 constexpr int multi_min_blocks()
 {
-  return C ? 3 : 4;
+  return (C || (DOT == kDotPair && Z <= 0)) ? 3 : 4;
 }
 
 template <typename VT2, int V, int W, int Z, class A, int MODE, int DOT, bool C>
-__global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const VT2* t0,
+__global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_vec(Op op, const VT2* t0,
                                                      const VT2* __restrict__ t1, VT2* out,
                                                      const VT2* __restrict__ left, Dot dot)
 {
@@ -889,13 +946,14 @@ __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const
     const int v0 = (int)(g % kTps) * W;
     const size_t base = (size_t)i * V + v0;
     const double p = op.pot[i];
-    double2 x[W];
-    ldw<W>(t1 + base, x);
+    VT2 x[W];  // T_{k-1} as stored; the pair mode reads it again after the row
+    ldw_raw<W>(t1 + base, x);
     double tr[W], ti[W];
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-      tr[k] = A::mul(p, x[k].x);
-      ti[k] = A::mul(p, x[k].y);
+      const double2 xk = widen(x[k]);
+      tr[k] = A::mul(p, xk.x);
+      ti[k] = A::mul(p, xk.y);
     }
     if constexpr (kPre) {
       hop_row_w<V, W, (Z > 0 ? Z : 1), A, C>(op, tb, i, v0, cur, t1, tr, ti);
@@ -955,13 +1013,14 @@ __global__ void __launch_bounds__(kBlock, kVecMinBlocks) k_step_vec(Op op, const
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         const double2 o = stored(out, r[k]);
+        const double2 xk = widen(x[k]);
         if constexpr (kExact) {
-          dot_term(re[2 * k], im[2 * k], o, o);
-          dot_term(re[2 * k + 1], im[2 * k + 1], o, x[k]);
+          dot_term_self(re[2 * k], o);
+          dot_term(re[2 * k + 1], im[2 * k + 1], o, xk);
         } else {
           re[2 * k].s = fma(o.x, o.x, fma(o.y, o.y, re[2 * k].s));
-          re[2 * k + 1].s = fma(o.x, x[k].x, fma(o.y, x[k].y, re[2 * k + 1].s));
-          im[2 * k + 1].s = fma(o.y, x[k].x, fma(-o.x, x[k].y, im[2 * k + 1].s));
+          re[2 * k + 1].s = fma(o.x, xk.x, fma(o.y, xk.y, re[2 * k + 1].s));
+          im[2 * k + 1].s = fma(o.y, xk.x, fma(-o.x, xk.y, im[2 * k + 1].s));
         }
       }
     }
@@ -986,6 +1045,10 @@ struct MultiDot {
   int tile_sites;
   int n_real;
   int blocks;              // grid of the step launch
+  // Host side only: 1 = leave the partials for a later k_tile_reduce over a window of
+  // steps (the launch writes the step's grid to *blocks_out).
+  int defer;
+  int* blocks_out;
 };
 
 enum { kDotOnly = 2 };
@@ -1038,7 +1101,7 @@ __device__ __forceinline__ void block_reduce_w(CSum (&re)[W], CSum (&im)[W], CSu
 // of that realisation; slots of realisations it never meets are zeroed.
 // k_tile_reduce then sums the blocks per realisation in fixed order.
 template <typename VT2, int V, int W, int Z, class A, int MODE, bool C, int DOT = kDotLeft>
-__global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op op, const VT2* t0,
+__global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_multi(Op op, const VT2* t0,
                                                        const VT2* __restrict__ t1, VT2* out,
                                                        const VT2* __restrict__ left, MultiDot md)
 {
@@ -1105,17 +1168,18 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
       const int v0 = (int)(g % kTps) * W;
       const size_t base = (size_t)i * V + v0;
       double2 r2[W];
-      double2 x[W];  // T_{k-1} (the pair mode's second product)
+      VT2 x[W];  // T_{k-1} as stored (the pair mode's second product)
       if constexpr (MODE == kDotOnly) {
         ldw<W>(t1 + base, r2);
       } else {
         const double p = op.pot[i];
-        ldw<W>(t1 + base, x);
+        ldw_raw<W>(t1 + base, x);
         double tr[W], ti[W];
 #pragma unroll
         for (int k = 0; k < W; ++k) {
-          tr[k] = A::mul(p, x[k].x);
-          ti[k] = A::mul(p, x[k].y);
+          const double2 xk = widen(x[k]);
+          tr[k] = A::mul(p, xk.x);
+          ti[k] = A::mul(p, xk.y);
         }
         if constexpr (kPre) {
           hop_row_w<V, W, (Z > 0 ? Z : 1), A, C>(op, tb, i, v0, cur, t1, tr, ti);
@@ -1174,13 +1238,14 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
 #pragma unroll
         for (int k = 0; k < W; ++k) {
           const double2 o = stored(out, r2[k]);
+          const double2 xk = widen(x[k]);
           if constexpr (kExact) {
-            dot_term(re[2 * k], im[2 * k], o, o);
-            dot_term(re[2 * k + 1], im[2 * k + 1], o, x[k]);
+            dot_term_self(re[2 * k], o);
+            dot_term(re[2 * k + 1], im[2 * k + 1], o, xk);
           } else {
             re[2 * k].s = fma(o.x, o.x, fma(o.y, o.y, re[2 * k].s));
-            re[2 * k + 1].s = fma(o.x, x[k].x, fma(o.y, x[k].y, re[2 * k + 1].s));
-            im[2 * k + 1].s = fma(o.y, x[k].x, fma(-o.x, x[k].y, im[2 * k + 1].s));
+            re[2 * k + 1].s = fma(o.x, xk.x, fma(o.y, xk.y, re[2 * k + 1].s));
+            im[2 * k + 1].s = fma(o.y, xk.x, fma(-o.x, xk.y, im[2 * k + 1].s));
           }
         }
       }
@@ -1198,16 +1263,20 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C>()) k_step_multi(Op
   }
 }
 
-// Per-realisation moments of a batch step: block p sums the slots of pair
-// p = (r, v) over the step's blocks in fixed order and writes mu[p].
+// Per-realisation moments of batch steps: block (p, j) sums the slots of pair
+// p = (r, v) of step j over the step's blocks in fixed order and writes
+// mu[j * pairs + p]. Step j's slots start j * row_stride doubles into md.partials: one
+// launch reduces one step (gridDim.y = 1) or a window of deferred steps, with the same
+// sums in the same order either way.
 template <int V>
-__global__ void __launch_bounds__(kBlock) k_tile_reduce(MultiDot md)
+__global__ void __launch_bounds__(kBlock) k_tile_reduce(MultiDot md, size_t row_stride)
 {
   const int p = blockIdx.x;
   const int pairs = md.n_real * V;
+  const double* row = md.partials + (size_t)blockIdx.y * row_stride;
   CSum re{0.0, 0.0}, im{0.0, 0.0};
   for (int b = threadIdx.x; b < md.blocks; b += kBlock) {
-    const double* q = md.partials + ((size_t)b * pairs + p) * 4;
+    const double* q = row + ((size_t)b * pairs + p) * 4;
     csum_merge(re, CSum{q[0], q[1]});
     csum_merge(im, CSum{q[2], q[3]});
   }
@@ -1231,7 +1300,8 @@ __global__ void __launch_bounds__(kBlock) k_tile_reduce(MultiDot md)
       csum_merge(a, CSum{sh[w][0], sh[w][1]});
       csum_merge(b, CSum{sh[w][2], sh[w][3]});
     }
-    md.mu[p] = make_double2(__dadd_rn(a.s, a.c), __dadd_rn(b.s, b.c));
+    md.mu[(size_t)blockIdx.y * pairs + p] =
+      make_double2(__dadd_rn(a.s, a.c), __dadd_rn(b.s, b.c));
   }
 }
 

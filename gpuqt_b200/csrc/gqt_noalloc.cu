@@ -25,7 +25,8 @@ static __device__ __align__(256) unsigned char g_step_scratch[kScratchBytes];
 
 // Per-device set-up, kept in fixed tables so that no call allocates.
 constexpr int kMaxDevices = 64;
-constexpr int kKernels = 3 * 4 * 2;  // V in {1, 4, 16} x Z in {3, 4, 6, any} x mode
+// V in {1, 4, 16} x Z in {3, 4, 6, any} x mode x operator format (ELL arrays, coded)
+constexpr int kKernels = 3 * 4 * 2 * 2;
 std::mutex g_setup_mu;
 void* g_scratch_addr[kMaxDevices];
 int g_sms[kMaxDevices];
@@ -35,42 +36,50 @@ int v_index(int nvec) { return nvec == 1 ? 0 : nvec == 4 ? 1 : 2; }
 
 int z_index(int z) { return z == 3 ? 0 : z == 4 ? 1 : z == 6 ? 2 : 3; }
 
-template <int V, int Z, int MODE>
+template <int V, int Z, int MODE, bool C>
 const void* kernel_of()
 {
-  return (const void*)gqt::k_step<double2, V, Z, ExactArith, MODE, true, false>;
+  return (const void*)gqt::k_step<double2, V, Z, ExactArith, MODE, true, C>;
 }
 
-template <int V, int MODE>
+template <int V, int MODE, bool C>
 const void* kernel_for_z(int z)
 {
   switch (z_index(z)) {
     case 0:
-      return kernel_of<V, 3, MODE>();
+      return kernel_of<V, 3, MODE, C>();
     case 1:
-      return kernel_of<V, 4, MODE>();
+      return kernel_of<V, 4, MODE, C>();
     case 2:
-      return kernel_of<V, 6, MODE>();
+      return kernel_of<V, 6, MODE, C>();
     default:
-      return kernel_of<V, 0, MODE>();
+      return kernel_of<V, 0, MODE, C>();
   }
 }
 
-const void* kernel_for(int nvec, int z, int mode)
+template <bool C>
+const void* kernel_for_c(int nvec, int z, int mode)
 {
   switch (v_index(nvec)) {
     case 0:
-      return mode == 0 ? kernel_for_z<1, kApply>(z) : kernel_for_z<1, kCheb>(z);
+      return mode == 0 ? kernel_for_z<1, kApply, C>(z) : kernel_for_z<1, kCheb, C>(z);
     case 1:
-      return mode == 0 ? kernel_for_z<4, kApply>(z) : kernel_for_z<4, kCheb>(z);
+      return mode == 0 ? kernel_for_z<4, kApply, C>(z) : kernel_for_z<4, kCheb, C>(z);
     default:
-      return mode == 0 ? kernel_for_z<16, kApply>(z) : kernel_for_z<16, kCheb>(z);
+      return mode == 0 ? kernel_for_z<16, kApply, C>(z) : kernel_for_z<16, kCheb, C>(z);
   }
 }
 
+const void* kernel_for(int nvec, int z, int mode, bool coded)
+{
+  return coded ? kernel_for_c<true>(nvec, z, mode) : kernel_for_c<false>(nvec, z, mode);
+}
+
 // Once per device, with that device current: the array's device address (host code
-// sees only a host-side stand-in under its name) and the launch limits.
-gqt_status setup(int dev, int nvec, int z, int mode, int* blocks_per_sm)
+// sees only a host-side stand-in under its name) and the launch limits. A coded
+// kernel's limit is taken with the largest operator table in shared memory, so the
+// grid never exceeds the blocks that are resident at once.
+gqt_status setup(int dev, int nvec, int z, int mode, bool coded, int* blocks_per_sm)
 {
   std::lock_guard<std::mutex> lock(g_setup_mu);
   if (!g_scratch_addr[dev]) {
@@ -85,11 +94,12 @@ gqt_status setup(int dev, int nvec, int z, int mode, int* blocks_per_sm)
     g_sms[dev] = sms > 0 ? sms : 1;
     g_scratch_addr[dev] = p;
   }
-  const int k = (v_index(nvec) * 4 + z_index(z)) * 2 + mode;
+  const int k = ((v_index(nvec) * 4 + z_index(z)) * 2 + mode) * 2 + (coded ? 1 : 0);
   if (g_blocks_per_sm[dev][k] == 0) {
     int b = 0;
-    cudaError_t e =
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel_for(nvec, z, mode), kBlock, 0);
+    const size_t smem = coded ? (size_t)GQT_MAX_CODES * 28 : 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &b, kernel_for(nvec, z, mode, coded), kBlock, smem);
     if (e != cudaSuccess)
       return gqt::cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__,
                             __LINE__);
@@ -99,28 +109,39 @@ gqt_status setup(int dev, int nvec, int z, int mode, int* blocks_per_sm)
   return GQT_OK;
 }
 
+template <int V, int MODE, bool C>
+void launch_c(int grid, cudaStream_t s, const Op& op, const double2* t0, const double2* t1,
+              double2* out, const double2* left, const Dot& d)
+{
+  const size_t smem = gqt::op_smem_bytes(op);  // the coded table; 0 on the ELL arrays
+  switch (z_index(op.z)) {
+    case 0:
+      gqt::k_step<double2, V, 3, ExactArith, MODE, true, C><<<grid, kBlock, smem, s>>>(
+        op, t0, t1, out, left, d);
+      break;
+    case 1:
+      gqt::k_step<double2, V, 4, ExactArith, MODE, true, C><<<grid, kBlock, smem, s>>>(
+        op, t0, t1, out, left, d);
+      break;
+    case 2:
+      gqt::k_step<double2, V, 6, ExactArith, MODE, true, C><<<grid, kBlock, smem, s>>>(
+        op, t0, t1, out, left, d);
+      break;
+    default:
+      gqt::k_step<double2, V, 0, ExactArith, MODE, true, C><<<grid, kBlock, smem, s>>>(
+        op, t0, t1, out, left, d);
+      break;
+  }
+}
+
 template <int V, int MODE>
 void launch(int grid, cudaStream_t s, const Op& op, const double2* t0, const double2* t1,
             double2* out, const double2* left, const Dot& d)
 {
-  switch (z_index(op.z)) {
-    case 0:
-      gqt::k_step<double2, V, 3, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
-                                                                                 out, left, d);
-      break;
-    case 1:
-      gqt::k_step<double2, V, 4, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
-                                                                                 out, left, d);
-      break;
-    case 2:
-      gqt::k_step<double2, V, 6, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
-                                                                                 out, left, d);
-      break;
-    default:
-      gqt::k_step<double2, V, 0, ExactArith, MODE, true, false><<<grid, kBlock, 0, s>>>(op, t0, t1,
-                                                                                 out, left, d);
-      break;
-  }
+  if (op.code)
+    launch_c<V, MODE, true>(grid, s, op, t0, t1, out, left, d);
+  else
+    launch_c<V, MODE, false>(grid, s, op, t0, t1, out, left, d);
 }
 
 }  // namespace
@@ -147,6 +168,10 @@ extern "C" gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, con
     return gqt::fail(GQT_ERR_ARG, "%s: %d vectors per call is not an FP64 form", w, nvec);
   if (out->data == t1->data)
     return gqt::fail(GQT_ERR_ARG, "%s: out must not alias t1", w);
+  // The pipelined step loads the next element's left value before this element's out
+  // is stored; with left == out the moment would depend on the loop shape.
+  if (out->data == left->data)
+    return gqt::fail(GQT_ERR_ARG, "%s: out must not alias left", w);
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess)
@@ -155,7 +180,8 @@ extern "C" gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, con
     return gqt::fail(GQT_ERR_ARG, "%s: device %d beyond the %d the tables hold", w, dev,
                      kMaxDevices);
   int bps = 0;
-  GQT_TRY(setup(dev, nvec, h->z, mode, &bps));
+  const bool coded = h->use_codes && h->code;
+  GQT_TRY(setup(dev, nvec, h->z, mode, coded, &bps));
 
   // Grid: as many blocks as are resident at once and as the elements need, capped so
   // that the block partials fit the static array.
@@ -185,7 +211,14 @@ extern "C" gqt_status gqt_chebyshev_step_noalloc(const gqt_ham* h, int mode, con
   if (e != cudaSuccess)
     return gqt::cuda_fail(e, "cudaMemsetAsync(counter)", __FILE__, __LINE__);
 
-  Op op{};  // the ELL arrays (no coded table: this launch has no dynamic shared memory)
+  Op op{};  // the operator in the Hamiltonian's format (coded table or ELL arrays)
+  if (coded) {
+    op.code = h->code;
+    op.code_delta = h->code_delta;
+    op.code_hop = h->code_hop;
+    op.code_xx = h->code_xx;
+    op.n_codes = h->n_codes;
+  }
   op.n = h->n;
   op.z = h->z;
   op.uniform = h->uniform;

@@ -324,35 +324,65 @@ extern "C" gqt_status gqt_vec_download(const gqt_vec* v, double* re, double* im)
   GQT_TRY(stage_alloc(&stage, 2 * count * sizeof(double)));
   gqt_status st = f->deinterleave(v->n, v->nvec, v->data, stage, stage + count);
   if (st == GQT_OK) {
-    // Through a pinned bounce buffer of kBounce doubles per device, chunk by chunk: a
-    // plain DMA and a host copy, not the driver's staging path for pageable memory,
-    // with the pinned memory bounded whatever the vector size.
-    constexpr size_t kBounce = (size_t)1 << 20;  // 8 MiB
+    // Through a pinned bounce buffer per device (two halves of kHalf doubles), chunk by
+    // chunk: a plain DMA and a host copy, not the driver's staging path for pageable
+    // memory, with the pinned memory bounded whatever the vector size. Chunk k + 1's
+    // DMA into one half runs while the host copies chunk k out of the other.
+    constexpr size_t kHalf = (size_t)1 << 19;  // 4 MiB
+    struct Bounce {
+      double* buf = nullptr;  // 2 * kHalf doubles
+      cudaEvent_t done[2] = {nullptr, nullptr};
+    };
     static std::mutex mu;
-    static std::unordered_map<int, double*> bounce;
+    static std::unordered_map<int, Bounce> bounce;
     int dev = 0;
     cudaGetDevice(&dev);
     std::lock_guard<std::mutex> lock(mu);
-    double*& b = bounce[dev];
+    Bounce& b = bounce[dev];
     cudaError_t e = cudaSuccess;
-    if (!b)
-      e = cudaMallocHost((void**)&b, kBounce * sizeof(double));
-    for (int part = 0; part < 2 && e == cudaSuccess; ++part) {
-      const double* src = stage + part * count;
-      double* dst = part ? im : re;
-      for (size_t off = 0; off < count && e == cudaSuccess; off += kBounce) {
-        const size_t len = count - off < kBounce ? count - off : kBounce;
-        e = cudaMemcpyAsync(b, src + off, len * sizeof(double), cudaMemcpyDeviceToHost,
-                            t_stream);
-        if (e == cudaSuccess)
-          e = cudaStreamSynchronize(t_stream);
-        if (e == cudaSuccess)
-          std::memcpy(dst + off, b, len * sizeof(double));
+    if (!b.buf) {
+      e = cudaMallocHost((void**)&b.buf, 2 * kHalf * sizeof(double));
+      if (e != cudaSuccess)
+        b.buf = nullptr;
+    }
+    for (int h = 0; h < 2 && e == cudaSuccess; ++h) {
+      if (!b.done[h]) {
+        e = cudaEventCreateWithFlags(&b.done[h], cudaEventDisableTiming);
+        if (e != cudaSuccess)
+          b.done[h] = nullptr;
       }
     }
+    struct Chunk {
+      const double* src;
+      double* dst;
+      size_t len;
+    };
+    std::vector<Chunk> chunks;
+    for (int part = 0; part < 2; ++part)
+      for (size_t off = 0; off < count; off += kHalf)
+        chunks.push_back({stage + part * count + off, (part ? im : re) + off,
+                          count - off < kHalf ? count - off : kHalf});
+    auto issue = [&](size_t k) {
+      const int h = (int)(k % 2);
+      cudaError_t r = cudaMemcpyAsync(b.buf + h * kHalf, chunks[k].src,
+                                      chunks[k].len * sizeof(double), cudaMemcpyDeviceToHost,
+                                      t_stream);
+      return r == cudaSuccess ? cudaEventRecord(b.done[h], t_stream) : r;
+    };
+    if (e == cudaSuccess && !chunks.empty())
+      e = issue(0);
+    for (size_t k = 0; k < chunks.size() && e == cudaSuccess; ++k) {
+      // The other half's host copy (chunk k - 1) finished in the previous iteration.
+      if (k + 1 < chunks.size())
+        e = issue(k + 1);
+      if (e == cudaSuccess)
+        e = cudaEventSynchronize(b.done[k % 2]);
+      if (e == cudaSuccess)
+        std::memcpy(chunks[k].dst, b.buf + (k % 2) * kHalf, chunks[k].len * sizeof(double));
+    }
     if (e != cudaSuccess) {
-      if (!b)
-        bounce.erase(dev);
+      // Leave the device's buffer usable (or absent) for the next call.
+      cudaStreamSynchronize(t_stream);
       st = cuda_fail(e, "download", __FILE__, __LINE__);
     }
   }
@@ -405,7 +435,7 @@ gqt_ham::~gqt_ham()
   cudaFree(hop);
   cudaFree(xx);
   cudaFree(pot);
-  cudaFree(tile_first);
+  cudaFree(tile_first_all);  // tile_first points into it
   cudaFree(code);
   cudaFree(code_delta);
   cudaFree(code_hop);
@@ -774,20 +804,62 @@ extern "C" gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count,
   // Each model is pre-divided by its own E_max, so the operator is applied with 1.
   GQT_TRY(upload_packed(P, 1.0, has_xx, h));
   h->n_real = count;
-  h->tile_sites = tile;
-  h->n_tiles = (int)(total / tile);
   h->real_offset = offset;
   for (int r = 0; r < count; ++r) {
     h->real_n.push_back(descs[r].n);
     h->real_emax.push_back(descs[r].energy_max);
   }
-  std::vector<int> first(count + 1);
-  for (int r = 0; r <= count; ++r)
-    first[r] = offset[r] / tile;
-  GQT_CUDA(cudaMalloc(&h->tile_first, first.size() * sizeof(int)));
-  GQT_CUDA(cudaMemcpy(h->tile_first, first.data(), first.size() * sizeof(int),
+  // The first tile of each model for every tile size the step can run with.
+  std::vector<int> first((size_t)kBatchTiles * (count + 1));
+  for (int k = 0; k < kBatchTiles; ++k)
+    for (int r = 0; r <= count; ++r)
+      first[(size_t)k * (count + 1) + r] = offset[r] / kBatchTileSizes[k];
+  GQT_CUDA(cudaMalloc(&h->tile_first_all, first.size() * sizeof(int)));
+  GQT_CUDA(cudaMemcpy(h->tile_first_all, first.data(), first.size() * sizeof(int),
                       cudaMemcpyHostToDevice));
+  GQT_TRY(batch_set_tile(h, kBatchTileSizes[0]));
   *out = guard.release();
+  return GQT_OK;
+}
+
+namespace gqt {
+
+gqt_status batch_set_tile(gqt_ham* h, int tile)
+{
+  for (int k = 0; k < kBatchTiles; ++k) {
+    if (kBatchTileSizes[k] != tile)
+      continue;
+    if (h->tile_sites != tile && h->ws) {
+      // Graphs captured so far launch the other tiling.
+      cudaStreamSynchronize(t_stream);
+      for (auto& kv : h->ws->graphs)
+        cudaGraphExecDestroy(kv.second);
+      h->ws->graphs.clear();
+    }
+    h->tile_sites = tile;
+    h->n_tiles = h->n / tile;
+    h->tile_first = h->tile_first_all + (size_t)k * (h->n_real + 1);
+    return GQT_OK;
+  }
+  return fail(GQT_ERR_ARG, "batch tile: %d sites is not one of 256, 512, 1024", tile);
+}
+
+}  // namespace gqt
+
+extern "C" gqt_status gqt_ham_set_batch_tile(gqt_ham* h, int tile_sites)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_batch_tile: null handle");
+  if (h->n_real < 2 || !h->tile_first_all)
+    return fail(GQT_ERR_STATE, "gqt_ham_set_batch_tile: not a realisation batch");
+  return batch_set_tile(h, tile_sites);
+}
+
+extern "C" gqt_status gqt_ham_batch_tile(const gqt_ham* h, int* tile_sites)
+{
+  if (!h || !tile_sites)
+    return fail(GQT_ERR_ARG, "gqt_ham_batch_tile: null argument");
+  *tile_sites = h->n_real > 1 ? h->tile_sites : 0;
   return GQT_OK;
 }
 

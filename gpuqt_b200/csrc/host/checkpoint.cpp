@@ -13,7 +13,9 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <fcntl.h>
 #include <sys/stat.h>
+#include <unistd.h>
 
 #include "gpuqt.h"
 #include "lsqt/model.h"
@@ -33,6 +35,17 @@ uint64_t fnv1a(const void* data, size_t n, uint64_t h = 1469598103934665603ull)
     h *= 1099511628211ull;
   }
   return h;
+}
+
+// Flush a file, or a directory's entries (dir = true), to disk; nothing if it does not
+// exist yet (an output file the run has not reached).
+void sync_path(const std::string& p, bool dir)
+{
+  const int fd = ::open(p.c_str(), dir ? (O_RDONLY | O_DIRECTORY) : O_RDONLY);
+  if (fd < 0)
+    return;
+  ::fsync(fd);
+  ::close(fd);
 }
 
 struct Writer {
@@ -155,16 +168,34 @@ void save_checkpoint(const std::string& path, const Checkpoint& ck)
     w.raw(s.data(), s.size() * sizeof(real));
   }
   w.put<uint64_t>(fnv1a(w.buf.data(), w.buf.size()));
+  // Durable order: the output rows the checkpoint counts, then the checkpoint's own
+  // bytes, then its name. A crash at any point leaves either the previous checkpoint
+  // or this one, each matching output files at least as long as it records.
+  const size_t slash = path.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? "" : path.substr(0, slash + 1);
+  for (const auto& f : ck.files)
+    sync_path(dir + f, false);
   const std::string tmp = path + ".tmp";
-  {
-    std::ofstream out(tmp, std::ios::binary | std::ios::trunc);
-    out.write(w.buf.data(), (std::streamsize)w.buf.size());
-    out.flush();
-    if (!out)
+  const int fd = ::open(tmp.c_str(), O_WRONLY | O_CREAT | O_TRUNC, 0644);
+  if (fd < 0)
+    die("Error: cannot write " + tmp, GQT_ERR_IO);
+  size_t done = 0;
+  while (done < w.buf.size()) {
+    const ssize_t k = ::write(fd, w.buf.data() + done, w.buf.size() - done);
+    if (k <= 0) {
+      ::close(fd);
       die("Error: cannot write " + tmp, GQT_ERR_IO);
+    }
+    done += (size_t)k;
   }
+  if (::fsync(fd) != 0) {
+    ::close(fd);
+    die("Error: cannot flush " + tmp + " to disk", GQT_ERR_IO);
+  }
+  ::close(fd);
   if (std::rename(tmp.c_str(), path.c_str()) != 0)
     die("Error: cannot rename " + tmp + " to " + path, GQT_ERR_IO);
+  sync_path(dir.empty() ? "." : dir, true);
 }
 
 bool load_checkpoint(const std::string& path, Checkpoint& ck)

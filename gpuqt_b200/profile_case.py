@@ -5,7 +5,9 @@
 Builds the workload's lattice, then runs `sets` moment sets of `moments` moments in
 one arithmetic form: fp64 (plain, one vector), fp32v1, or fp32vV (V vectors per
 launch, FP32 storage), with the operator in the coded format (the default where the
-lattice has one) or in the plain ELL arrays (`--format ell`). Prints one JSON line
+lattice has one) or in the plain ELL arrays (`--format ell`). With `--doubled` each
+set is a symmetric moment set from half the Chebyshev steps (gqt_moments_doubled: the
+step kernels in pair mode); the rate counts the moments produced. Prints one JSON line
 with the measured rate.
 """
 from __future__ import annotations
@@ -31,6 +33,8 @@ def main() -> None:
     ap.add_argument("--format", default="default", choices=["default", "ell", "coded"])
     ap.add_argument("--autotune", action="store_true",
                     help="let the autotuner pick the shape for this vector count first")
+    ap.add_argument("--doubled", action="store_true",
+                    help="symmetric moment sets from half the steps (pair-mode kernels)")
     args = ap.parse_args()
 
     import torch
@@ -70,12 +74,18 @@ def main() -> None:
         mu = torch.empty(2 * args.moments * V * R, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream()
         g.set_stream(stream.cuda_stream)
-        g.moments_device(H, X, X, args.moments, mu.data_ptr())
+        if args.doubled:
+            def one():
+                g.moments_doubled_device(H, X, args.moments, mu.data_ptr())
+        else:
+            def one():
+                g.moments_device(H, X, X, args.moments, mu.data_ptr())
+        one()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         for _ in range(args.sets):
-            g.moments_device(H, X, X, args.moments, mu.data_ptr())
+            one()
         b.record(stream)
         torch.cuda.synchronize()
         s = a.elapsed_time(b) / 1e3
@@ -83,6 +93,7 @@ def main() -> None:
                           "format": "coded" if H.format == g.FORMAT_CODED else "ell",
                           "n_codes": H.n_codes,
                           "moments": args.moments, "sets": args.sets, "autotune": tuned,
+                          "doubled": args.doubled,
                           "site_moments_per_s": V * sites * args.moments * args.sets / s}))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

@@ -10,11 +10,13 @@
  * reference checkout). Device work is issued on the calling thread's current stream
  * (gqt_set_stream); calls that return host data synchronise that stream.
  *
- * Layout on the device (owned by the handles, see DESIGN.md):
+ * Layout on the device (owned by the handles):
  *   vectors      interleaved complex, [site][vector] (double2 or float2)
  *   Hamiltonian  ELL column-major [m*n + i]: int32 neighbour index, double2 hopping,
  *                double xx; double on-site potential [n]; int32 row length [n] only
- *                when rows are ragged.
+ *                when rows are ragged; where the entries take at most GQT_MAX_CODES
+ *                distinct values, also a one-byte code per entry and the table of
+ *                those values (the coded format).
  */
 #ifndef GPUQT_H
 #define GPUQT_H
@@ -110,17 +112,26 @@ gqt_status gqt_ham_format(const gqt_ham* h, int* format, int* n_codes);
  * gqt_kernel_polynomial apply the scaled operator; the evolution and current
  * entry points are rejected (their Bessel coefficients depend on each model's
  * energy_max). */
-#define GQT_BATCH_TILE_SITES 256
+#define GQT_BATCH_TILE_SITES 1024
 #define GQT_MAX_REALISATIONS 32
 gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count, gqt_ham** out);
+/* The batch step hands out tiles of 256, 512 or 1024 consecutive sites (each divides
+ * the padding, so a tile never straddles two models); gqt_autotune_nvec picks the
+ * fastest, gqt_ham_set_batch_tile sets one (GQT_ERR_STATE on a single model), and
+ * gqt_ham_batch_tile reports the one in use (0 on a single model). Moments agree
+ * between tile sizes to rounding (the per-block sums group differently). */
+gqt_status gqt_ham_set_batch_tile(gqt_ham* h, int tile_sites);
+gqt_status gqt_ham_batch_tile(const gqt_ham* h, int* tile_sites);
 gqt_status gqt_ham_realisations(const gqt_ham* h, int* count);
 gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
                                double* energy_max);
 /* Project autotuner for the batched moment loop: times n_moments Chebyshev steps for
  * each candidate number of vectors per launch (a supported nvec of `precision`) on
  * this Hamiltonian and returns the one with the highest site-moments/s in *best
- * (rates[k] receives candidate k's rate; may be NULL). Allocates and frees its own
- * probe vectors. */
+ * (rates[k] receives candidate k's best rate; may be NULL). For every candidate it
+ * also picks the vector-block shape of the step (vectors per thread, FP32: 4 or 2)
+ * and, on a realisation batch, the tile size (256, 512 or 1024 sites), keeping the
+ * fastest for later launches. Allocates and frees its own probe vectors. */
 gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_moments,
                              const int* candidates, int n_candidates, int* best,
                              double* rates);
@@ -302,11 +313,13 @@ gqt_status gqt_lsqt_run(const char* input_dir, int precision, int verbose, long 
  * GQT_NOALLOC_SCRATCH_BYTES that every GPU loading the library holds until exit.
  *
  *   mode 0: out = H t1 / E_max           (t0 ignored; the first step)
- *   mode 1: out = 2 H t1 / E_max - t0    (out may alias t0)
+ *   mode 1: out = 2 H t1 / E_max - t0    (out may alias t0; never t1 or left)
  *   mu_dev: device array of nvec double2 receiving <left|out> (re, im)
  *
  * FP64 vectors only (the reference's arithmetic; out is bit-identical to
- * gqt_apply / gqt_kernel_polynomial). The launch uses at most
+ * gqt_apply / gqt_kernel_polynomial), the operator read in the Hamiltonian's current
+ * format (gqt_ham_set_format; the coded table goes to shared memory, no allocation).
+ * The launch uses at most
  * GQT_NOALLOC_SCRATCH_BYTES / (32 * nvec) blocks; a call whose reduction would need
  * more scratch than that is rejected with GQT_ERR_ARG. The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) and must come before
