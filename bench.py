@@ -482,6 +482,8 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         im = np.stack([v[1] for v in vecs])
         X = g.Vector.from_host(re, im, nvec=V, precision=g.FP32)
         mu = torch.empty(2 * M * V, dtype=torch.float64, device="cuda")
+        # the vector-block shape (vectors per thread) as the autotuner picks it
+        shape = g.autotune_nvec(H, g.FP32, 20, [V])[1] if V >= 4 else None
         for _ in range(2):
             g.moments_device(H, X, X, M, mu.data_ptr())
         reps = max(2, min(args.steps, 5))
@@ -500,6 +502,7 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         out[f"fp32_v{V}"] = {"site_moments_per_s": rate, "vectors_per_launch": V,
                              "achieved_gbs": ach, "frac": ach / hbm_peak,
                              "bytes_per_site_moment": fp32_bytes_per_site_vector(V, coded=coded),
+                             "autotune_rate": shape,
                              "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32, i32))}
         if V == 16 and coded:
             # the same form on the plain ELL arrays
@@ -683,6 +686,8 @@ def measure_cubic(g, torch, tmp, stream, hbm_peak, vectors=16):
     X = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
                            nvec=vectors, precision=g.FP32)
     mu32 = torch.empty(2 * M * vectors, dtype=torch.float64, device="cuda")
+    # the vector-block shape as the autotuner picks it on this lattice
+    g.autotune_nvec(H, g.FP32, 20, [vectors])
     ms32 = timed(lambda: g.moments_device(H, X, X, M, mu32.data_ptr()))
     mu_h = mu32.view(M, vectors, 2).cpu().numpy()
     dos = P.compare(g, m, (r64, i64), (mu_h[:, 0, 0].copy(), mu_h[:, 0, 1].copy()))

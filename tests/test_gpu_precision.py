@@ -1,7 +1,19 @@
 """The FP32-storage form against the FP64 form on the precision workload (honeycomb
-graphene, 4,194,304 sites, 5000 moments): DOS and VAC within 1e-6 of the FP64
-result (largest per-energy deviation relative to the peak). Four VAC steps here; the
-full 20-step report is `python -m gpuqt_b200.precision_report`."""
+graphene, 4,194,304 sites, W = 1.5, seed 5, 5000 moments), DOS and all 20 VAC steps.
+
+The error measures, per moment set (precision_report.compare):
+  energy_rel_peak_max     max over energies |X32(E) - X64(E)| / max_E |X64(E)|, the
+                          norm-wise relative error of the DOS or VAC row; bound 1e-6
+                          for the DOS and every VAC step
+  energy_rel_in_band_max  max |X32(E) - X64(E)| / |X64(E)| over energies where
+                          |X64(E)| > 1 % of the row's peak (pointwise); bound 1e-6 for
+                          the DOS. For the VAC at late correlation times the row is a
+                          small difference of large moments and the FP32 rounding inside
+                          the recurrence (not the rounding of the start vectors) reaches
+                          a few 1e-6 pointwise; the bound asserted is 1e-5 and the
+                          measured value is printed
+  moment_rel_mu0_max      max_m |mu32_m - mu64_m| / |mu64_0|; bound 1e-7
+"""
 from __future__ import annotations
 
 import json
@@ -13,9 +25,14 @@ from gpuqt_b200 import precision_report
 pytestmark = pytest.mark.gpu
 
 
-def test_graphene4m_fp32_within_1e6():
-    r = precision_report.report("graphene4m", vac_steps=4)
+@pytest.mark.slow
+def test_graphene4m_fp32_against_fp64_dos_and_20_vac_steps():
+    r = precision_report.report("graphene4m", vac_steps=20)
     print(json.dumps(r))
-    assert r["sites"] == 4194304 and r["moments"] == 5000
+    assert r["sites"] == 4194304 and r["moments"] == 5000 and r["vac_steps"] == 20
     assert r["dos"]["energy_rel_peak_max"] <= 1e-6
+    assert r["dos"]["energy_rel_in_band_max"] <= 1e-6
+    assert r["dos"]["moment_rel_mu0_max"] <= 1e-7
     assert r["vac"]["energy_rel_peak_max"] <= 1e-6
+    assert r["vac"]["energy_rel_in_band_max"] <= 1e-5
+    assert r["vac"]["moment_rel_mu0_max"] <= 1e-7
