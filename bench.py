@@ -69,6 +69,12 @@ def fp32_bytes_per_site_vector(V, z=Z, coded=True):
     return (z * entry_bytes(coded) + 8) / V + 4 * 8
 
 
+# FP32X storage: FP32 plus a BF16 residual, 12 bytes per complex element, in all four
+# streams (the loop's copy of left is FP32X too).
+def fp32x_bytes_per_site_vector(V, z=Z, coded=True):
+    return (z * entry_bytes(coded) + 8) / V + 4 * 12
+
+
 # A step of a symmetric (doubled) moment set reads T_{k-1} and T_{k-2} and writes T_k
 # (no left stream) and yields two moments.
 def fp64_pair_bytes_per_site_step(z=Z, coded=True):
@@ -523,6 +529,33 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
                                    "bytes_per_site_moment":
                                        fp32_bytes_per_site_vector(V, coded=False)}
 
+    # The FP32X form (FP32 storage with a BF16 residual), 16 vectors per launch, from
+    # the same 16 FP64 vectors; error of vector 0 against its FP64 moments.
+    vecs = [phi] + [m.initial_state() for _ in range(15)]
+    X16 = g.Vector.from_host(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]),
+                             nvec=16)
+    mu = torch.empty(2 * M * 16, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        g.moments_device(H, X16, X16, M, mu.data_ptr(), precision=g.FP32X)
+    reps = max(2, min(args.steps, 5))
+    a, b = ev()
+    a.record(stream)
+    for _ in range(reps):
+        g.moments_device(H, X16, X16, M, mu.data_ptr(), precision=g.FP32X)
+    b.record(stream)
+    torch.cuda.synchronize()
+    s = a.elapsed_time(b) / 1e3
+    bx = fp32x_bytes_per_site_vector(16, coded=coded)
+    ach = bx * 16 * n * M * reps / s / 1e9
+    mh = mu.view(M, 16, 2).cpu().numpy()
+    from gpuqt_b200 import precision_report as P
+    out["fp32x_v16"] = {"site_moments_per_s": 16 * n * M * reps / s, "vectors_per_launch": 16,
+                        "achieved_gbs": ach, "frac": ach / hbm_peak,
+                        "bytes_per_site_moment": bx,
+                        "dos_err_vs_fp64": P.compare(g, m, (r64, i64),
+                                                     (mh[:, 0, 0].copy(), mh[:, 0, 1].copy()))}
+    del X16, mu
+
     def fp64_rate(fmt):
         # plain FP64 rate from a short timed loop, for the ratios
         H.set_format(fmt)
@@ -542,6 +575,8 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
     H.set_format(default)
     for k in [k for k in out if k.startswith("fp32")]:
         out[k]["speedup_vs_fp64"] = out[k]["site_moments_per_s"] / rate64
+    out["fp32x_v16"]["byte_ceiling_vs_fp64"] = (fp64_bytes_per_site(coded=coded) /
+                                                fp32x_bytes_per_site_vector(16, coded=coded))
     out["fp64_v1_site_moments_per_s"] = rate64
 
     # Symmetric moment sets from half the Chebyshev steps (gqt_moments_doubled): the
@@ -611,6 +646,8 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         "frac_fp64_doubled": out["fp64_doubled"]["frac"],
         "frac_fp32_v16_doubled": out["fp32_v16_doubled"]["frac"],
         "dos_err_fp32_v16": d32["dos_err_vs_fp64"],
+        "speedup_fp32x_v16_direct": out["fp32x_v16"]["speedup_vs_fp64"],
+        "frac_fp32x_v16_direct": out["fp32x_v16"]["frac"],
         "met_like_for_like": bool(max(ratio_direct, ratio_dbl) >= 3.0 and
                                   d32["frac"] >= 0.7 and out["fp64_v1"]["frac"] >= 0.7),
         "note": "while both forms are HBM-bound the like-for-like ratio is capped by "

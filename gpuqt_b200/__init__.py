@@ -25,6 +25,7 @@ CLI_PATH = os.path.join(HERE, "lib", "lsqt_b200")
 
 FP64 = 0
 FP32 = 1
+FP32X = 2  # moment recurrence only: FP32 storage with a BF16 residual
 FORMAT_ELL = 0    # the reference's ELL arrays
 FORMAT_CODED = 1  # one byte per ELL entry into a table of the distinct entries
 
@@ -532,9 +533,16 @@ def autotune_nvec(H: Hamiltonian, precision: int, n_moments: int, candidates):
 
 
 def moments_device(H: Hamiltonian, left: Vector, right: Vector, n_moments: int,
-                   mu_dev_ptr: int) -> None:
-    """Moments into device memory (n_moments * nvec double2, moment-major); async."""
-    _call("gqt_moments_device", H.h, left.h, right.h, n_moments, ctypes.c_void_p(mu_dev_ptr))
+                   mu_dev_ptr: int, precision: int | None = None) -> None:
+    """Moments into device memory (n_moments * nvec double2, moment-major); async.
+    `precision` runs the recurrence in another form than the vectors'
+    (gqt_moments_device_form)."""
+    if precision is None:
+        _call("gqt_moments_device", H.h, left.h, right.h, n_moments,
+              ctypes.c_void_p(mu_dev_ptr))
+    else:
+        _call("gqt_moments_device_form", H.h, left.h, right.h, n_moments, precision,
+              ctypes.c_void_p(mu_dev_ptr))
 
 
 def evolve(H: Hamiltonian, direction: int, dt_scaled: float, state: Vector) -> None:

@@ -8,6 +8,7 @@ when a source or any header under csrc/ or include/ is newer. Run as
 from __future__ import annotations
 
 import os
+import shlex
 import shutil
 import subprocess
 import sys
@@ -27,12 +28,15 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["gqt_runtime.cu", "gqt_algo.cu", "gqt_forms_fp64.cu", "gqt_forms_fp32.cu",
+              "gqt_forms_fp32x.cu",
               "gqt_forms_fp64_coded.cu", "gqt_forms_fp32_coded.cu", "gqt_noalloc.cu"]
 CPP_SOURCES = ["host/model.cpp", "host/vector_ham.cpp", "host/sigma.cpp", "host/lsqt.cpp",
                "host/checkpoint.cpp", "host/batch_run.cpp"]
 
 NVCC_FLAGS = ARCH + ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
                      "-Xptxas", "-v", f"-I{INCLUDE}", f"-I{CSRC}"]
+# Extra nvcc flags (e.g. -DGQT_VEC_STREAMS=1 to build a pipeline variant for timing).
+NVCC_FLAGS += shlex.split(os.environ.get("GQT_NVCC_FLAGS", ""))
 # -ffp-contract=off keeps the host arithmetic (random draws, Chebyshev sums) in the
 # reference's rounding: every product and sum rounded on its own.
 CXX_FLAGS = ["-std=c++17", "-O2", "-fPIC", "-ffp-contract=off", "-Wall", f"-I{INCLUDE}",

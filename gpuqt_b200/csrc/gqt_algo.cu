@@ -24,6 +24,7 @@ Workspace::~Workspace()
   cudaFree(mu);
   cudaFreeHost(mu_host);
   cudaFree(pairs);
+  cudaFree(xarena);
   if (ev_in)
     cudaEventDestroy(ev_in);
   if (ev_out)
@@ -73,6 +74,29 @@ gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out)
     GQT_CUDA(cudaMemset(ws.dot.counter, 0, 2 * sizeof(unsigned)));
   }
   *out = &ws.dot;
+  return GQT_OK;
+}
+
+gqt_status ws_arena_x(Workspace& ws, size_t elems)
+{
+  // Slots start on 64-element boundaries, so every W-element access (W <= 4) of the
+  // FP32 parts and of the residuals is aligned to its width.
+  const size_t slot = (elems + 63) / 64 * 64;
+  if (ws.xslot >= slot && ws.xarena)
+    return GQT_OK;
+  cudaStreamSynchronize(stream());
+  // Graphs captured with the old arena can never run again.
+  for (auto& kv : ws.graphs)
+    cudaGraphExecDestroy(kv.second);
+  ws.graphs.clear();
+  cudaFree(ws.xarena);
+  ws.xarena = nullptr;
+  ws.xslot = 0;
+  GQT_CUDA(cudaMalloc(&ws.xarena, (size_t)kXSlots * slot * 12));
+  ws.xslot = slot;
+  const uintptr_t base = reinterpret_cast<uintptr_t>(ws.xarena);  // 256-byte aligned
+  const uintptr_t res = base + (uintptr_t)kXSlots * slot * 8;
+  ws.xlo = res - base / 2;
   return GQT_OK;
 }
 
@@ -298,7 +322,8 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
                            const gqt_vec* right, int M, double2* mu, void* A, void* B,
                            DotScratch* ds)
 {
-  const Op op = make_op(h, right->nvec);
+  Op op = make_op(h, right->nvec);
+  op.xlo = right->xlo;
   const int V = right->nvec;
   const size_t total = (size_t)h->n * V;
   if (h->n_real > 1) {
@@ -323,7 +348,7 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
     }
     return GQT_OK;
   }
-  Dot d{ds->partials, ds->counter, mu};
+  Dot d{ds->partials, ds->counter, mu, 0, right->xlo};
   GQT_TRY(f->dot(total, right->data, left->data, d));
   if (M < 2)
     return GQT_OK;
@@ -350,7 +375,8 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
 gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_vec* phi, int M,
                                 double2* mu, double2* pairs, void* A, void* B, DotScratch* ds)
 {
-  const Op op = make_op(h, phi->nvec);
+  Op op = make_op(h, phi->nvec);
+  op.xlo = phi->xlo;
   const int V = phi->nvec;
   const size_t total = (size_t)h->n * V;
   if (h->n_real > 1) {
@@ -381,7 +407,7 @@ gqt_status moment_launches_pair(const gqt_ham* h, const FormOps* f, const gqt_ve
     GQT_CUDA(cudaGetLastError());
     return GQT_OK;
   }
-  Dot d{ds->partials, ds->counter, pairs};
+  Dot d{ds->partials, ds->counter, pairs, 0, phi->xlo};
   GQT_TRY(f->dot(total, phi->data, phi->data, d));
   const int K = M / 2;
   if (K >= 1) {
@@ -640,9 +666,15 @@ static gqt_status moments_prepare(const gqt_ham* h, const gqt_vec* left, const g
   if (!*f)
     return GQT_ERR_ARG;
   Workspace& ws = *h->ws;
-  const size_t bytes = right->bytes;
-  GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
-  GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
+  if (right->precision == GQT_FP32X) {
+    // the recurrence's two buffers share the inputs' arena (one residual map)
+    *A = ws_xslot(ws, 2);
+    *B = ws_xslot(ws, 3);
+  } else {
+    const size_t bytes = right->bytes;
+    GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 0, A));
+    GQT_TRY(ws_vector(ws, right->precision, right->nvec, bytes, 1, B));
+  }
   // Block partials: [grid][R][V][4] doubles for a batch, [grid][V][4] otherwise, followed
   // by the slab of a window of deferred moments.
   const int results = h->n_real * right->nvec;
@@ -791,6 +823,29 @@ static gqt_status moments_form_run(const gqt_ham* h, const gqt_vec* left, const 
     return fail(GQT_ERR_ARG, "%s: form %d has no %d-vector launch", w, precision, right->nvec);
   if (left->n != right->n || left->nvec != right->nvec)
     return fail(GQT_ERR_ARG, "%s: left and right differ in size or count", w);
+  if (precision == GQT_FP32X) {
+    // Copies of left and right in the FP32X arena (slots 1 and 0); the recurrence runs
+    // in slots 2 and 3.
+    if (h->n_real > 1)
+      return fail(GQT_ERR_STATE, "%s: the FP32X form runs on one model, not a batch", w);
+    if (right->precision == GQT_FP32X || left->precision == GQT_FP32X)
+      return fail(GQT_ERR_ARG, "%s: FP32X vectors are internal to the moment loop", w);
+    GQT_TRY(check_pair(h, right, w));
+    Workspace& ws = *h->ws;
+    const size_t elems = (size_t)right->n * right->nvec;
+    GQT_TRY(ws_arena_x(ws, elems));
+    const bool same = left->data == right->data;
+    GQT_TRY(convert_to_x(elems, right->precision, right->data, ws_xslot(ws, 0), ws.xlo));
+    if (!same)
+      GQT_TRY(convert_to_x(elems, left->precision, left->data, ws_xslot(ws, 1), ws.xlo));
+    gqt_vec R = *right, L = *left;
+    R.precision = L.precision = GQT_FP32X;
+    R.bytes = L.bytes = elems * 8;
+    R.xlo = L.xlo = ws.xlo;
+    R.data = ws_xslot(ws, 0);
+    L.data = same ? R.data : ws_xslot(ws, 1);
+    return moments_run(h, &L, &R, M, mu_dev, pair, w);
+  }
   // The converted copies live in workspace slots 4 and 5 of the target form (slots
   // 0-3 are the recurrence and evolution temporaries).
   Workspace& ws = *h->ws;

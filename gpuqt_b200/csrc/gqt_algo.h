@@ -28,6 +28,12 @@ struct Workspace {
   cudaEvent_t ev_in = nullptr, ev_out = nullptr;
   double2* pairs = nullptr;  // pair products of the symmetric moment loop
   size_t pairs_bytes = 0;
+  // FP32X moment loops: one arena of kXSlots slots (right, left, T_a, T_b) of `xslot`
+  // elements each, the FP32 parts of all slots first, then their BF16 residuals, so
+  // that the residual of the element at p lies at xlo + p / 2.
+  unsigned char* xarena = nullptr;
+  size_t xslot = 0;
+  uintptr_t xlo = 0;
   // Instantiated moment loops: (left, right, n_moments, mu, precision, nvec, loop),
   // loop 0 the direct one, 1 the symmetric (pair) one.
   using GraphKey = std::tuple<const void*, const void*, int, void*, int, int, int>;
@@ -41,6 +47,11 @@ Workspace* new_workspace();
 // The i-th temporary vector of a form (n * nvec elements of elem bytes).
 gqt_status ws_vector(Workspace& ws, int precision, int nvec, size_t bytes, int i, void** out);
 gqt_status ws_dot(Workspace& ws, size_t doubles, DotScratch** out);
+// The FP32X arena for `elems` elements per slot; slot k's FP32 part is returned by
+// ws_xslot(ws, k).
+constexpr int kXSlots = 4;
+gqt_status ws_arena_x(Workspace& ws, size_t elems);
+inline void* ws_xslot(const Workspace& ws, int k) { return ws.xarena + (size_t)k * ws.xslot * 8; }
 // Moments per window of deferred grid stages for `results` sums per moment.
 int defer_window(int results);
 

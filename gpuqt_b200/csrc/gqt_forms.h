@@ -93,6 +93,10 @@ struct FormOps {
 
 const FormOps* forms_fp64(int nvec);
 const FormOps* forms_fp32(int nvec);
+// GQT_FP32X: moment loops only (dot, step, step_pair; nvec 1, 4, 16).
+const FormOps* forms_fp32x(int nvec);
+// src (GQT_FP64 or GQT_FP32 storage, `total` elements) into FP32X storage at dst.
+gqt_status convert_to_x(size_t total, int from, const void* src, void* dst, uintptr_t xlo);
 // The coded format's operator kernels (gqt_forms_fp64_coded.cu, gqt_forms_fp32_coded.cu).
 OpFns op_fns_fp64_coded(int nvec);
 OpFns op_fns_fp32_coded(int nvec);
@@ -102,6 +106,8 @@ inline const FormOps* form_ops(int precision, int nvec)
     return forms_fp64(nvec);
   if (precision == GQT_FP32)
     return forms_fp32(nvec);
+  if (precision == GQT_FP32X)
+    return forms_fp32x(nvec);
   return nullptr;
 }
 

@@ -78,7 +78,16 @@ gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
   return GQT_OK;
 }
 
-// Vectors a thread advances per step launch: 4 float2 (two 16-byte loads) or 2 double2.
+// Storage types with FP32 elements (float2; xf2, FP32 with a BF16 residual).
+template <typename VT2>
+struct Fp32Like
+    : std::integral_constant<bool, std::is_same<VT2, float2>::value ||
+                                       std::is_same<VT2, xf2>::value> {
+};
+
+// Vectors a thread advances per step launch: 4 float2 (two 16-byte loads), 2 double2,
+// or 2 FP32X elements (a 16-byte load and an 8-byte residual load; at 4 the residuals'
+// registers spilled on rows of 4 and 6).
 template <typename VT2, int V>
 constexpr int vectors_per_thread()
 {
@@ -96,7 +105,7 @@ struct OpImpl {
   // double2. The pair mode keeps three FP64 sums per vector and T_{k-1} until the end
   // of an item; at the direct step's width (4 float2, 2 double2) that spilled 120-250
   // bytes per thread at the step's register budget.
-  static constexpr int WP = std::is_same<VT2, float2>::value ? (V < 2 ? V : 2) : 1;
+  static constexpr int WP = Fp32Like<VT2>::value ? (V < 2 ? V : 2) : 1;
 
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)

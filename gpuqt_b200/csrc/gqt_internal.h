@@ -66,6 +66,9 @@ struct gqt_vec {
   void* data = nullptr;  // double2 or float2, [site][vector]
   size_t bytes = 0;
   int device = 0;
+  // GQT_FP32X copies (workspace only): data holds the FP32 parts, the residual of the
+  // element at p lies at xlo + p / 2
+  uintptr_t xlo = 0;
 };
 
 struct gqt_ham {

@@ -21,6 +21,7 @@
 // block partials in fixed block order. The result does not depend on timing.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -50,6 +51,7 @@ struct Op {
   const double2* __restrict__ code_hop;
   const double* __restrict__ code_xx;
   int n_codes;
+  uintptr_t xlo;  // FP32X storage: residual of the element at p is at xlo + p / 2
 };
 
 struct Dot {
@@ -59,6 +61,7 @@ struct Dot {
   // 1: the block writes its partials and leaves; k_slab_combine combines them later
   // in the same order (block 0 records gridDim.x in counter[1]).
   int defer;
+  uintptr_t xlo;  // FP32X storage of the vectors read (as Op::xlo)
 };
 
 // ------------------------------------------------------------------ operator entries
@@ -195,14 +198,15 @@ struct FastArith {
 };
 
 // ------------------------------------------------------------------ storage
-__device__ __forceinline__ double2 ld(const double2* p) { return *p; }
-__device__ __forceinline__ double2 ld(const float2* p)
+// Every load and store takes `xlo`, which only the FP32X form (below) reads.
+__device__ __forceinline__ double2 ld(const double2* p, uintptr_t = 0) { return *p; }
+__device__ __forceinline__ double2 ld(const float2* p, uintptr_t = 0)
 {
   float2 f = *p;
   return make_double2((double)f.x, (double)f.y);
 }
-__device__ __forceinline__ void st(double2* p, double2 v) { *p = v; }
-__device__ __forceinline__ void st(float2* p, double2 v)
+__device__ __forceinline__ void st(double2* p, double2 v, uintptr_t = 0) { *p = v; }
+__device__ __forceinline__ void st(float2* p, double2 v, uintptr_t = 0)
 {
   *p = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
 }
@@ -211,6 +215,57 @@ __device__ __forceinline__ double2 stored(const double2*, double2 v) { return v;
 __device__ __forceinline__ double2 stored(const float2*, double2 v)
 {
   return make_double2((double)__double2float_rn(v.x), (double)__double2float_rn(v.y));
+}
+
+// FP32X storage (the moment recurrence of the GQT_FP32X form): an element v is kept as
+// hi = RN_fp32(v) and lo = RN_bf16(v - hi), 12 bytes per complex element instead of
+// FP64's 16, with about 32 significant bits. hi is an xf2 at address p; its residual,
+// a bf16 pair, lies at xlo + p / 2: the vectors of a moment loop are carved from one
+// workspace arena whose residual region is the FP32 region's image under that map, so
+// the residuals of consecutive elements are consecutive 4-byte words and W elements'
+// residuals are one 4W-byte load.
+struct __align__(8) xf2 {
+  float x, y;
+};
+__device__ __forceinline__ const __nv_bfloat162* xres(const xf2* p, uintptr_t xlo)
+{
+  return reinterpret_cast<const __nv_bfloat162*>(xlo + reinterpret_cast<uintptr_t>(p) / 2);
+}
+__device__ __forceinline__ __nv_bfloat162* xres(xf2* p, uintptr_t xlo)
+{
+  return reinterpret_cast<__nv_bfloat162*>(xlo + reinterpret_cast<uintptr_t>(p) / 2);
+}
+__device__ __forceinline__ double2 xjoin(float hx, float hy, __nv_bfloat162 l)
+{
+  const float2 lf = __bfloat1622float2(l);
+  return make_double2((double)hx + (double)lf.x, (double)hy + (double)lf.y);
+}
+// hi and the rounded residual of v
+__device__ __forceinline__ void xsplit(double2 v, float2& h, __nv_bfloat162& l)
+{
+  h = make_float2(__double2float_rn(v.x), __double2float_rn(v.y));
+  l = __floats2bfloat162_rn(__double2float_rn(v.x - (double)h.x),
+                            __double2float_rn(v.y - (double)h.y));
+}
+__device__ __forceinline__ double2 ld(const xf2* p, uintptr_t xlo)
+{
+  const xf2 h = *p;
+  return xjoin(h.x, h.y, *xres(p, xlo));
+}
+__device__ __forceinline__ void st(xf2* p, double2 v, uintptr_t xlo)
+{
+  float2 h;
+  __nv_bfloat162 l;
+  xsplit(v, h, l);
+  *reinterpret_cast<float2*>(p) = h;
+  *xres(p, xlo) = l;
+}
+__device__ __forceinline__ double2 stored(const xf2*, double2 v)
+{
+  float2 h;
+  __nv_bfloat162 l;
+  xsplit(v, h, l);
+  return xjoin(h.x, h.y, l);
 }
 
 // ------------------------------------------------------------------ compensated sums
@@ -397,7 +452,7 @@ __device__ __forceinline__ void dot_finish(CSum re, CSum im, const Dot& dot)
 // W consecutive complex elements of one site, as wide loads: two float2 per float4,
 // one double2 each. Offsets are multiples of W elements, so the loads are aligned.
 template <int W>
-__device__ __forceinline__ void ldw(const float2* p, double2 (&o)[W])
+__device__ __forceinline__ void ldw(const float2* p, double2 (&o)[W], uintptr_t = 0)
 {
   if constexpr (W == 1) {
     o[0] = ld(p);
@@ -412,7 +467,7 @@ __device__ __forceinline__ void ldw(const float2* p, double2 (&o)[W])
 }
 
 template <int W>
-__device__ __forceinline__ void ldw(const double2* p, double2 (&o)[W])
+__device__ __forceinline__ void ldw(const double2* p, double2 (&o)[W], uintptr_t = 0)
 {
 #pragma unroll
   for (int k = 0; k < W; ++k)
@@ -420,7 +475,7 @@ __device__ __forceinline__ void ldw(const double2* p, double2 (&o)[W])
 }
 
 template <int W>
-__device__ __forceinline__ void stw(float2* p, const double2 (&v)[W])
+__device__ __forceinline__ void stw(float2* p, const double2 (&v)[W], uintptr_t = 0)
 {
   if constexpr (W == 1) {
     st(p, v[0]);
@@ -434,18 +489,104 @@ __device__ __forceinline__ void stw(float2* p, const double2 (&v)[W])
 }
 
 template <int W>
-__device__ __forceinline__ void stw(double2* p, const double2 (&v)[W])
+__device__ __forceinline__ void stw(double2* p, const double2 (&v)[W], uintptr_t = 0)
 {
 #pragma unroll
   for (int k = 0; k < W; ++k)
     p[k] = v[k];
 }
 
+// W consecutive FP32X elements: the hi parts as float4 loads, the residuals as one
+// 4W-byte load (W = 1, 2 or 4; the offsets are multiples of W elements).
+template <int W>
+__device__ __forceinline__ void ldw_hi(const xf2* p, float2 (&h)[W])
+{
+  if constexpr (W == 1) {
+    h[0] = *reinterpret_cast<const float2*>(p);
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k) {
+      const float4 f = reinterpret_cast<const float4*>(p)[k];
+      h[2 * k] = make_float2(f.x, f.y);
+      h[2 * k + 1] = make_float2(f.z, f.w);
+    }
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void xres_ld(const xf2* p, uintptr_t xlo, __nv_bfloat162 (&l)[W])
+{
+  const __nv_bfloat162* r = xres(p, xlo);
+  if constexpr (W == 4) {
+    const uint4 u = *reinterpret_cast<const uint4*>(r);
+    const unsigned w[4] = {u.x, u.y, u.z, u.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      l[k] = *reinterpret_cast<const __nv_bfloat162*>(&w[k]);
+  } else if constexpr (W == 2) {
+    const uint2 u = *reinterpret_cast<const uint2*>(r);
+    l[0] = *reinterpret_cast<const __nv_bfloat162*>(&u.x);
+    l[1] = *reinterpret_cast<const __nv_bfloat162*>(&u.y);
+  } else {
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      l[k] = r[k];
+  }
+}
+
+template <int W>
+__device__ __forceinline__ void ldw(const xf2* p, double2 (&o)[W], uintptr_t xlo)
+{
+  float2 h[W];
+  ldw_hi<W>(p, h);
+  __nv_bfloat162 l[W];
+  xres_ld<W>(p, xlo, l);
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    o[k] = xjoin(h[k].x, h[k].y, l[k]);
+}
+
+template <int W>
+__device__ __forceinline__ void stw(xf2* p, const double2 (&v)[W], uintptr_t xlo)
+{
+  float2 h[W];
+  __nv_bfloat162 l[W];
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    xsplit(v[k], h[k], l[k]);
+  if constexpr (W == 1) {
+    *reinterpret_cast<float2*>(p) = h[0];
+  } else {
+#pragma unroll
+    for (int k = 0; k < W / 2; ++k)
+      reinterpret_cast<float4*>(p)[k] = make_float4(h[2 * k].x, h[2 * k].y, h[2 * k + 1].x,
+                                                    h[2 * k + 1].y);
+  }
+  __nv_bfloat162* r = xres(p, xlo);
+  if constexpr (W == 4) {
+    uint4 u;
+    u.x = *reinterpret_cast<const unsigned*>(&l[0]);
+    u.y = *reinterpret_cast<const unsigned*>(&l[1]);
+    u.z = *reinterpret_cast<const unsigned*>(&l[2]);
+    u.w = *reinterpret_cast<const unsigned*>(&l[3]);
+    *reinterpret_cast<uint4*>(r) = u;
+  } else if constexpr (W == 2) {
+    uint2 u;
+    u.x = *reinterpret_cast<const unsigned*>(&l[0]);
+    u.y = *reinterpret_cast<const unsigned*>(&l[1]);
+    *reinterpret_cast<uint2*>(r) = u;
+  } else {
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      r[k] = l[k];
+  }
+}
+
 // W consecutive elements kept in their storage type (the same wide loads as ldw). A
 // value a kernel needs twice, far apart, costs half the registers as float2 and is
 // widened exactly at each use.
 template <int W>
-__device__ __forceinline__ void ldw_raw(const float2* p, float2 (&o)[W])
+__device__ __forceinline__ void ldw_raw(const float2* p, float2 (&o)[W], uintptr_t = 0)
 {
   if constexpr (W == 1) {
     o[0] = *p;
@@ -460,18 +601,46 @@ __device__ __forceinline__ void ldw_raw(const float2* p, float2 (&o)[W])
 }
 
 template <int W>
-__device__ __forceinline__ void ldw_raw(const double2* p, double2 (&o)[W])
+__device__ __forceinline__ void ldw_raw(const double2* p, double2 (&o)[W], uintptr_t = 0)
 {
 #pragma unroll
   for (int k = 0; k < W; ++k)
     o[k] = p[k];
 }
 
+// An FP32X element as stored: hi and its residual (12 bytes, three registers).
+struct xraw {
+  float2 h;
+  __nv_bfloat162 l;
+};
+template <int W>
+__device__ __forceinline__ void ldw_raw(const xf2* p, xraw (&o)[W], uintptr_t xlo)
+{
+  float2 h[W];
+  ldw_hi<W>(p, h);
+  __nv_bfloat162 l[W];
+  xres_ld<W>(p, xlo, l);
+#pragma unroll
+  for (int k = 0; k < W; ++k)
+    o[k] = xraw{h[k], l[k]};
+}
+
+// The register type ldw_raw fills for a storage type.
+template <typename VT2>
+struct Raw {
+  using type = VT2;
+};
+template <>
+struct Raw<xf2> {
+  using type = xraw;
+};
+
 __device__ __forceinline__ double2 widen(double2 v) { return v; }
 __device__ __forceinline__ double2 widen(float2 v)
 {
   return make_double2((double)v.x, (double)v.y);
 }
+__device__ __forceinline__ double2 widen(const xraw& v) { return xjoin(v.h.x, v.h.y, v.l); }
 
 // ------------------------------------------------------------------ the operator row
 // f(m) for the entries m < cnt of a row, unrolled when the bound Z is known.
@@ -504,7 +673,7 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
         int j, c;
         double2 h;
         ell_entry<C>(op, tb, e, i, j, h, c);
-        const double2 y = ld(x + (size_t)j * V + v);
+        const double2 y = ld(x + (size_t)j * V + v, op.xlo);
         tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
         ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
       }
@@ -515,7 +684,7 @@ __device__ __forceinline__ void hop_row(const Op& op, const Tables& tb, int i, i
       int j, c;
       double2 h;
       ell_entry<C>(op, tb, e, i, j, h, c);
-      const double2 y = ld(x + (size_t)j * V + v);
+      const double2 y = ld(x + (size_t)j * V + v, op.xlo);
       tr = A::add(tr, A::cre(h.x, h.y, y.x, y.y));
       ti = A::add(ti, A::cim(h.x, h.y, y.x, y.y));
     }
@@ -611,7 +780,7 @@ __device__ __forceinline__ void hop_row_pre(const Op& op, const Tables& tb, int 
 #pragma unroll
   for (int m = 0; m < Z; ++m)
     if (m < r.cnt)
-      y[m] = ld(x + (size_t)j[m] * V + v);
+      y[m] = ld(x + (size_t)j[m] * V + v, op.xlo);
 #pragma unroll
   for (int m = 0; m < Z; ++m) {
     if (m < r.cnt) {
@@ -648,7 +817,7 @@ __device__ __forceinline__ void hop_row_w(const Op& op, const Tables& tb, int i,
       double2 h;
       row_entry<C>(op, tb, i, m, r.idx[m], j, h);
       double2 y[W];
-      ldw<W>(x + (size_t)j * V + v0, y);
+      ldw<W>(x + (size_t)j * V + v0, y, op.xlo);
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
@@ -710,14 +879,14 @@ __device__ __forceinline__ void fetch_hops(const Op& op, int i, RowHop<Z>& r)
 // hop_row from a prefetched ELL row and its prefetched hoppings.
 template <int V, int Z, class A, typename VT2>
 __device__ __forceinline__ void hop_row_ahead(int v, const RowIdx<Z>& r, const RowHop<Z>& hr,
-                                              const VT2* __restrict__ x, double& tr,
-                                              double& ti)
+                                              const VT2* __restrict__ x, uintptr_t xlo,
+                                              double& tr, double& ti)
 {
   double2 y[Z];
 #pragma unroll
   for (int m = 0; m < Z; ++m)
     if (m < r.cnt)
-      y[m] = ld(x + (size_t)r.idx[m] * V + v);
+      y[m] = ld(x + (size_t)r.idx[m] * V + v, xlo);
 #pragma unroll
   for (int m = 0; m < Z; ++m) {
     if (m < r.cnt) {
@@ -739,13 +908,13 @@ __device__ __forceinline__ void fetch_streams(const Op& op, size_t g, const VT2*
                                               const VT2* __restrict__ left, Streams& s)
 {
   s.p = op.pot[g / V];
-  s.x = ld(t1 + g);
+  s.x = ld(t1 + g, op.xlo);
   s.y0 = make_double2(0.0, 0.0);
   s.l = s.y0;
   if constexpr (MODE == kCheb)
-    s.y0 = ld(t0 + g);
+    s.y0 = ld(t0 + g, op.xlo);
   if constexpr (DOT == kDotLeft)
-    s.l = ld(left + g);
+    s.l = ld(left + g, op.xlo);
 }
 
 // The fused moment terms of one element: o = T_k as stored, x = T_{k-1}, l = left.
@@ -822,7 +991,7 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z, DOT, C>()) k_step(O
       double tr = A::mul(s.p, s.x.x);
       double ti = A::mul(s.p, s.x.y);
       if constexpr (kHops)
-        hop_row_ahead<V, Z, A>(v, cur, hc, t1, tr, ti);
+        hop_row_ahead<V, Z, A>(v, cur, hc, t1, op.xlo, tr, ti);
       else
         hop_row_pre<V, Z, A, C>(op, tb, i, v, cur, t1, tr, ti);
       tr = A::scale(tr, op);
@@ -832,7 +1001,7 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z, DOT, C>()) k_step(O
         ti = A::two_x_minus(ti, s.y0.y);
       }
       const double2 r = make_double2(tr, ti);
-      st(out + g, r);
+      st(out + g, r, op.xlo);
       step_dot<DOT>(re, im, stored(out, r), s.x, s.l);
       cur = nxt;
       hc = hn;
@@ -843,21 +1012,21 @@ __global__ void __launch_bounds__(kBlock, step_min_blocks<Z, DOT, C>()) k_step(O
       const int i = (int)(g / V);
       const int v = (int)(g % V);
       const double p = op.pot[i];
-      const double2 x = ld(t1 + g);
+      const double2 x = ld(t1 + g, op.xlo);
       double tr = A::mul(p, x.x);
       double ti = A::mul(p, x.y);
       hop_row<V, Z, A, C>(op, tb, i, v, t1, tr, ti);
       tr = A::scale(tr, op);
       ti = A::scale(ti, op);
       if constexpr (MODE == kCheb) {
-        const double2 y0 = ld(t0 + g);
+        const double2 y0 = ld(t0 + g, op.xlo);
         tr = A::two_x_minus(tr, y0.x);
         ti = A::two_x_minus(ti, y0.y);
       }
       const double2 r = make_double2(tr, ti);
-      st(out + g, r);
+      st(out + g, r, op.xlo);
       if constexpr (DOT == kDotLeft)
-        step_dot<DOT>(re, im, stored(out, r), x, ld(left + g));
+        step_dot<DOT>(re, im, stored(out, r), x, ld(left + g, op.xlo));
       else
         step_dot<DOT>(re, im, stored(out, r), x, x);
     }
@@ -877,7 +1046,7 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
   CSum re{0.0, 0.0}, im{0.0, 0.0};
   for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
        g += (size_t)gridDim.x * kBlock)
-    dot_term(re, im, ld(state + g), ld(left + g));
+    dot_term(re, im, ld(state + g, dot.xlo), ld(left + g, dot.xlo));
   dot_finish<V>(re, im, dot);
 }
 
@@ -890,10 +1059,49 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t total, const VT2* __restr
 // compiler's own choice: k_step_vec at 4 (64 registers: +9 % for 16 FP32 vectors on
 // graphene, +7 % on cubic, +17 % for 32 vectors on the ELL arrays); k_step_multi at 3
 // with the coded table, 4 on the ELL arrays.
+// The streamed inputs of one k_step_vec item (W vectors of one site) in their storage
+// type: potential, T_{k-1}, T_{k-2} (kCheb) and left (kDotLeft).
+template <typename VT2, int W, int MODE, int DOT>
+struct VecStreams {
+  double p;
+  typename Raw<VT2>::type x[W];
+  typename Raw<VT2>::type y0[MODE == kCheb ? W : 1];
+  typename Raw<VT2>::type l[DOT == kDotLeft ? W : 1];
+};
+
+template <int V, int W, int TPS, int MODE, int DOT, typename VT2>
+__device__ __forceinline__ void fetch_vec_streams(const Op& op, size_t g, const VT2* t0,
+                                                  const VT2* __restrict__ t1,
+                                                  const VT2* __restrict__ left,
+                                                  VecStreams<VT2, W, MODE, DOT>& s)
+{
+  const int i = (int)(g / TPS);
+  const size_t base = (size_t)i * V + (size_t)(g % TPS) * W;
+  s.p = op.pot[i];
+  ldw_raw<W>(t1 + base, s.x, op.xlo);
+  if constexpr (MODE == kCheb)
+    ldw_raw<W>(t0 + base, s.y0, op.xlo);
+  if constexpr (DOT == kDotLeft)
+    ldw_raw<W>(left + base, s.l, op.xlo);
+}
+
+// Whether k_step_vec loads an item's streamed inputs one grid-stride iteration ahead
+// (with its row), so that they are in flight during the previous item's gathers: the
+// in-place store of T_k (over T_{k-2}) keeps the compiler from hoisting them itself.
+// GQT_VEC_STREAMS = 0 or 1 at compile time forces it off or on.
+#ifndef GQT_VEC_STREAMS
+#define GQT_VEC_STREAMS 0
+#endif
+template <int DOT>
+__host__ __device__ constexpr bool vec_streams_ahead()
+{
+  return GQT_VEC_STREAMS > 0 && DOT == kDotPair;
+}
+
 // The pair mode of a symmetric set keeps three sums per vector and T_{k-1} for the whole
-// item: rows of unknown length (Z = 0) and the FP64 form on rows of six take 3 blocks
-// per SM there (at 4 they spilled 40-140 bytes per thread), the FP64 form on rows of
-// unknown length 2 (12-24 bytes at 3).
+// item: rows of unknown length (Z = 0), and the FP64 and FP32X forms on rows of six,
+// take 3 blocks per SM there (at 4 they spilled 16-140 bytes per thread), the FP64
+// form on rows of unknown length 2 (12-24 bytes at 3).
 constexpr int kVecMinBlocks = 4;
 template <typename VT2, int Z, int DOT>
 constexpr int vec_min_blocks()
@@ -901,10 +1109,12 @@ constexpr int vec_min_blocks()
   constexpr bool f64 = std::is_same<VT2, double2>::value;
   if constexpr (DOT != kDotPair)
     return kVecMinBlocks;
+  else if constexpr (vec_streams_ahead<DOT>() && Z > 0)
+    return 3;  // the look-ahead's second set of streams
   else if constexpr (Z <= 0)
     return f64 ? 2 : 3;
   else
-    return (Z >= 6 && f64) ? 3 : kVecMinBlocks;
+    return (Z >= 6 && !std::is_same<VT2, float2>::value) ? 3 : kVecMinBlocks;
 }
 template <bool C, int Z = 4, int DOT = kDotLeft>
 constexpr int multi_min_blocks()
@@ -927,27 +1137,44 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
 #pragma unroll
   for (int k = 0; k < kSums; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
-  // Pipelined as in k_step where the policy says so: the next item's row first.
+  // Pipelined as in k_step where the policy says so: the next item's row first, and
+  // (kPreS) its streamed inputs too.
   constexpr bool kPre = Z > 0 && pipelined<kPipeStepVec, C, VT2, Z>();
+  constexpr bool kPreS = kPre && vec_streams_ahead<DOT>();
   RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
+  VecStreams<VT2, W, MODE, DOT> sc;
   const size_t stride = (size_t)gridDim.x * kBlock;
   size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x;
   if constexpr (kPre) {
-    if (g < items)
+    if (g < items) {
       fetch_row<(Z > 0 ? Z : 1), C>(op, (int)(g / kTps), cur);
+      if constexpr (kPreS)
+        fetch_vec_streams<V, W, kTps, MODE, DOT>(op, g, t0, t1, left, sc);
+    }
   }
   for (; g < items; g += stride) {
+    VecStreams<VT2, W, MODE, DOT> s;
+    if constexpr (kPreS)
+      s = sc;
     if constexpr (kPre) {
       nxt = cur;
-      if (g + stride < items)
+      if (g + stride < items) {
         fetch_row<(Z > 0 ? Z : 1), C>(op, (int)((g + stride) / kTps), nxt);
+        if constexpr (kPreS)
+          fetch_vec_streams<V, W, kTps, MODE, DOT>(op, g + stride, t0, t1, left, sc);
+      }
     }
     const int i = (int)(g / kTps);
     const int v0 = (int)(g % kTps) * W;
     const size_t base = (size_t)i * V + v0;
-    const double p = op.pot[i];
-    VT2 x[W];  // T_{k-1} as stored; the pair mode reads it again after the row
-    ldw_raw<W>(t1 + base, x);
+    if constexpr (!kPreS) {
+      // without the look-ahead T_{k-2} and left are loaded late, each right before use
+      // (held across the gathers they cost 4-vector items 140-160 bytes of spills)
+      s.p = op.pot[i];
+      ldw_raw<W>(t1 + base, s.x, op.xlo);
+    }
+    const double p = s.p;
+    const auto& x = s.x;  // T_{k-1} as stored; the pair mode reads it again
     double tr[W], ti[W];
 #pragma unroll
     for (int k = 0; k < W; ++k) {
@@ -965,7 +1192,7 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
         double2 h;
         ell_entry<C>(op, tb, e, i, j, h, c);
         double2 y[W];
-        ldw<W>(t1 + (size_t)j * V + v0, y);
+        ldw<W>(t1 + (size_t)j * V + v0, y, op.xlo);
 #pragma unroll
         for (int k = 0; k < W; ++k) {
           tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
@@ -984,21 +1211,27 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
     }
     double2 r[W];
     if constexpr (MODE == kCheb) {
-      double2 y0[W];
-      ldw<W>(t0 + base, y0);
+      if constexpr (!kPreS)
+        ldw_raw<W>(t0 + base, s.y0, op.xlo);
 #pragma unroll
-      for (int k = 0; k < W; ++k)
-        r[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0[k].x),
-                            A::two_x_minus(A::scale(ti[k], op), y0[k].y));
+      for (int k = 0; k < W; ++k) {
+        const double2 y0 = widen(s.y0[k]);
+        r[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0.x),
+                            A::two_x_minus(A::scale(ti[k], op), y0.y));
+      }
     } else {
 #pragma unroll
       for (int k = 0; k < W; ++k)
         r[k] = make_double2(A::scale(tr[k], op), A::scale(ti[k], op));
     }
-    stw<W>(out + base, r);
+    stw<W>(out + base, r, op.xlo);
     if constexpr (DOT == kDotLeft) {
+      if constexpr (!kPreS)
+        ldw_raw<W>(left + base, s.l, op.xlo);
       double2 l[W];
-      ldw<W>(left + base, l);
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        l[k] = widen(s.l[k]);
 #pragma unroll
       for (int k = 0; k < W; ++k) {
         if constexpr (kExact) {
@@ -1672,6 +1905,16 @@ __global__ void __launch_bounds__(kBlock) k_convert(size_t total, const ST2* __r
   for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
        g += (size_t)gridDim.x * kBlock)
     st(dst + g, ld(src + g));
+}
+
+// dst = src into FP32X storage (the FP32X moment loop's copies of its input vectors).
+template <typename ST2>
+__global__ void __launch_bounds__(kBlock) k_to_x(size_t total, const ST2* __restrict__ src,
+                                                 xf2* __restrict__ dst, uintptr_t xlo)
+{
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < total;
+       g += (size_t)gridDim.x * kBlock)
+    st(dst + g, ld(src + g), xlo);
 }
 
 // FP64 accumulator -> FP32 state (end of an FP32-form evolution).

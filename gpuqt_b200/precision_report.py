@@ -2,12 +2,13 @@
 
     python -m gpuqt_b200.precision_report --workload graphene4m --vac-steps 20
 
-Runs the DOS moment set and the VAC moment sets (src/sigma.cu:278-327) in both forms
-for the first random-phase vector of the workload and prints one JSON line with, per
-quantity: the largest per-moment error relative to the moment (complex modulus), the
-largest per-moment error relative to mu_0, and the largest per-energy error of the
-damped Chebyshev sum relative to its peak (and relative to the value, over energies
-where the value exceeds 1 % of the peak).
+Runs the DOS moment set and the VAC moment sets (src/sigma.cu:278-327) in the FP64
+form and in the FP32-storage form (and, under "fp32x", in the FP32X form: FP32 storage
+with a BF16 residual) for the first random-phase vector of the workload and prints
+one JSON line with, per quantity: the largest per-moment error relative to the moment
+(complex modulus), the largest per-moment error relative to mu_0, and the largest
+per-energy error of the damped Chebyshev sum relative to its peak (and relative to the
+value, over energies where the value exceeds 1 % of the peak).
 """
 from __future__ import annotations
 
@@ -56,7 +57,8 @@ def vac_moments(g, model, H, phi, precision, steps):
     return out
 
 
-def report(workload: str, vac_steps: int, moments: int | None = None) -> dict:
+def report(workload: str, vac_steps: int, moments: int | None = None,
+           fp32x: bool = True) -> dict:
     import gpuqt_b200 as g
 
     tmp = tempfile.mkdtemp(prefix="gqt_prec_")
@@ -75,14 +77,21 @@ def report(workload: str, vac_steps: int, moments: int | None = None) -> dict:
                "moments": m.n_moments}
         x64 = g.Vector.from_host(*phi)
         x32 = g.Vector.from_host(*phi, precision=g.FP32)
-        out["dos"] = compare(g, m, g.moments(H, x64, x64, m.n_moments),
-                             g.moments(H, x32, x32, m.n_moments))
+        d64 = g.moments(H, x64, x64, m.n_moments)
+        out["dos"] = compare(g, m, d64, g.moments(H, x32, x32, m.n_moments))
         steps = min(vac_steps, m.n_steps) if m.n_steps else vac_steps
         a = vac_moments(g, m, H, phi, g.FP64, steps)
         b = vac_moments(g, m, H, phi, g.FP32, steps)
         per = [compare(g, m, a[k], b[k]) for k in range(steps)]
         out["vac_steps"] = steps
         out["vac"] = {k: max(p[k] for p in per) for k in per[0]}
+        if fp32x:
+            c = vac_moments(g, m, H, phi, g.FP32X, steps)
+            per = [compare(g, m, a[k], c[k]) for k in range(steps)]
+            out["fp32x"] = {
+                "dos": compare(g, m, d64, g.moments(H, x64, x64, m.n_moments,
+                                                    precision=g.FP32X)),
+                "vac": {k: max(p[k] for p in per) for k in per[0]}}
         return out
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

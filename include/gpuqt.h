@@ -42,7 +42,15 @@ enum {
 /* Arithmetic forms of a Hamiltonian/vector pair. */
 enum {
   GQT_FP64 = 0, /* plain: FP64 vectors, FP64 operator, reference operation order */
-  GQT_FP32 = 1  /* precision: FP32 vectors, FP64 operator and FP64 compensated sums */
+  GQT_FP32 = 1, /* precision: FP32 vectors, FP64 operator and FP64 compensated sums */
+  /* No counterpart in the reference. A form of the moment recurrence only (the
+   * precision argument of gqt_moments_form / _device_form / gqt_moments_doubled*, on
+   * FP64 or FP32 vectors of one model, 1, 4 or 16 per launch): each Chebyshev vector
+   * is stored as FP32 plus a BF16 residual (12 bytes per complex element against
+   * FP64's 16, about 32 significant bits), with the FP64 operator and FP64 sums.
+   * DOS and VAC agree with FP64 to about 1e-8 pointwise, where FP32 storage reaches a
+   * few 1e-6 at late VAC times. Vectors of this form cannot be created. */
+  GQT_FP32X = 2
 };
 
 typedef struct gqt_ham gqt_ham;

@@ -7,10 +7,21 @@ tests/golden/make_golden_large.py):
   cubic256    16,777,216 sites, z = 6: the first 200 DOS moments
 
 The host model builder must reproduce the reference's ELL arrays, hoppings, xx and
-Anderson potentials bit for bit (SHA-256 of each array; CPU), and the FP64 form every
-moment to 1e-12 relative (GPU), in both operator formats. At these sizes every thread
-of the step kernels runs several grid-stride iterations, which the small fixtures never
-reach, so the hand-over between elements is checked against the reference itself."""
+Anderson potentials bit for bit (SHA-256 of each array; CPU). The FP64 form's moments
+(GPU, both operator formats) must satisfy, for every m,
+
+    |mu_m - mu_ref,m| <= 1e-12 |mu_ref,m| + 2 max_k |Im mu_ref,k|.
+
+The second term is the reference's own rounding at this size: these moments
+<psi|T_m|psi> are real, so the imaginary parts of the reference's moments are the
+rounding noise of its sequential FP64 sum over millions of sites (6e-12 to 1.5e-11
+here). Its real parts carry noise of the same order, which exceeds 1e-12 of the
+smallest moments (|mu| = 0.25 to 3.4 of mu_0 = 2-4 million). The library's moments
+are bit-identical vectors summed in a different order (compensated), so the difference
+is the reference's rounding; the largest plain relative difference is printed. At
+these sizes every thread of the step kernels runs several grid-stride iterations, which
+the small fixtures never reach, so the hand-over between elements is checked against
+the reference itself."""
 from __future__ import annotations
 
 import hashlib
@@ -65,6 +76,14 @@ def _rel(mr, mi, rr, ri):
     return float(np.max(np.hypot(mr - rr, mi - ri) / np.hypot(rr, ri)))
 
 
+def _within(mr, mi, rr, ri):
+    """The per-moment bound above; returns (ok, plain relative max, noise floor)."""
+    floor = 2.0 * float(np.max(np.abs(ri)))
+    err = np.hypot(mr - rr, mi - ri)
+    ok = bool(np.all(err <= REL_FP64 * np.hypot(rr, ri) + floor))
+    return ok, _rel(mr, mi, rr, ri), floor
+
+
 @pytest.mark.gpu
 @pytest.mark.slow
 @pytest.mark.parametrize("name", LARGE)
@@ -79,7 +98,9 @@ def test_dos_moments_match_reference_build_at_size(name):
     for fmt in fmts:
         H.set_format(fmt)
         mr, mi = g.moments(H, x, x, m.n_moments)
-        assert _rel(mr, mi, rr, ri) <= REL_FP64, (name, fmt)
+        ok, rel, floor = _within(mr, mi, rr, ri)
+        print(name, fmt, "max relative difference", rel, "reference noise floor", floor)
+        assert ok, (name, fmt, rel, floor)
         got.append((mr, mi))
     if len(got) == 2:
         # the two formats hold the same doubles: identical vectors, moments to the order
@@ -104,7 +125,9 @@ def test_msd_moments_match_reference_build_at_size():
     g.evolvex(H, 1, ts[0] * m.energy_max, sx)
     for k in range(steps):
         mr, mi = g.moments(H, sx, sx, M)
-        assert _rel(mr, mi, ref["re"][k], ref["im"][k]) <= REL_FP64, k
+        ok, rel, floor = _within(mr, mi, ref["re"][k], ref["im"][k])
+        print("msd step", k, "max relative difference", rel, "reference noise floor", floor)
+        assert ok, (k, rel, floor)
         if k < steps - 1:
             dt = ts[k + 1] * m.energy_max
             copy.copy_from(state)
