@@ -78,6 +78,11 @@ gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
   return GQT_OK;
 }
 
+// FP32-element vectors per thread in pair mode (2; a build may set 4 for timing).
+#ifndef GQT_PAIR_W_FP32
+#define GQT_PAIR_W_FP32 2
+#endif
+
 // Storage types with FP32 elements (float2; xf2, FP32 with a BF16 residual).
 template <typename VT2>
 struct Fp32Like
@@ -105,7 +110,8 @@ struct OpImpl {
   // double2. The pair mode keeps three FP64 sums per vector and T_{k-1} until the end
   // of an item; at the direct step's width (4 float2, 2 double2) that spilled 120-250
   // bytes per thread at the step's register budget.
-  static constexpr int WP = Fp32Like<VT2>::value ? (V < 2 ? V : 2) : 1;
+  static constexpr int WP =
+    Fp32Like<VT2>::value ? (V < GQT_PAIR_W_FP32 ? V : GQT_PAIR_W_FP32) : 1;
 
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)

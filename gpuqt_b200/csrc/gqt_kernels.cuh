@@ -1090,12 +1090,24 @@ __device__ __forceinline__ void fetch_vec_streams(const Op& op, size_t g, const 
 // in-place store of T_k (over T_{k-2}) keeps the compiler from hoisting them itself.
 // GQT_VEC_STREAMS = 0 or 1 at compile time forces it off or on.
 #ifndef GQT_VEC_STREAMS
-#define GQT_VEC_STREAMS 0
+#define GQT_VEC_STREAMS 1
 #endif
-template <int DOT>
+// Whether the direct steps load left before storing T_k (left is read-only, but the
+// compiler cannot move its load above the store itself): 0 or 1 at compile time.
+#ifndef GQT_LEFT_EARLY
+#define GQT_LEFT_EARLY 0
+#endif
+// Blocks per SM of the pair-mode step on rows of known length (0: the defaults below; a
+// build may set it for timing).
+#ifndef GQT_PAIR_MINB
+#define GQT_PAIR_MINB 0
+#endif
+template <typename VT2, int DOT>
 __host__ __device__ constexpr bool vec_streams_ahead()
 {
-  return GQT_VEC_STREAMS > 0 && DOT == kDotPair;
+  // pair mode only (the direct step's 4-vector items spill holding a second set), and
+  // not for FP32X (its residuals' registers spill at the look-ahead's budget)
+  return GQT_VEC_STREAMS > 0 && DOT == kDotPair && !std::is_same<VT2, xf2>::value;
 }
 
 // The pair mode of a symmetric set keeps three sums per vector and T_{k-1} for the whole
@@ -1109,8 +1121,8 @@ constexpr int vec_min_blocks()
   constexpr bool f64 = std::is_same<VT2, double2>::value;
   if constexpr (DOT != kDotPair)
     return kVecMinBlocks;
-  else if constexpr (vec_streams_ahead<DOT>() && Z > 0)
-    return 3;  // the look-ahead's second set of streams
+  else if constexpr ((vec_streams_ahead<VT2, DOT>() || GQT_PAIR_MINB > 0) && Z > 0)
+    return GQT_PAIR_MINB > 0 ? GQT_PAIR_MINB : 3;  // the look-ahead's second set of streams
   else if constexpr (Z <= 0)
     return f64 ? 2 : 3;
   else
@@ -1140,7 +1152,7 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
   // Pipelined as in k_step where the policy says so: the next item's row first, and
   // (kPreS) its streamed inputs too.
   constexpr bool kPre = Z > 0 && pipelined<kPipeStepVec, C, VT2, Z>();
-  constexpr bool kPreS = kPre && vec_streams_ahead<DOT>();
+  constexpr bool kPreS = kPre && vec_streams_ahead<VT2, DOT>();
   RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
   VecStreams<VT2, W, MODE, DOT> sc;
   const size_t stride = (size_t)gridDim.x * kBlock;
@@ -1210,6 +1222,8 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
       }
     }
     double2 r[W];
+    if constexpr (DOT == kDotLeft && !kPreS && GQT_LEFT_EARLY)
+      ldw_raw<W>(left + base, s.l, op.xlo);
     if constexpr (MODE == kCheb) {
       if constexpr (!kPreS)
         ldw_raw<W>(t0 + base, s.y0, op.xlo);
@@ -1226,7 +1240,7 @@ __global__ void __launch_bounds__(kBlock, vec_min_blocks<VT2, Z, DOT>()) k_step_
     }
     stw<W>(out + base, r, op.xlo);
     if constexpr (DOT == kDotLeft) {
-      if constexpr (!kPreS)
+      if constexpr (!kPreS && !GQT_LEFT_EARLY)
         ldw_raw<W>(left + base, s.l, op.xlo);
       double2 l[W];
 #pragma unroll
@@ -1402,6 +1416,7 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_
       const size_t base = (size_t)i * V + v0;
       double2 r2[W];
       VT2 x[W];  // T_{k-1} as stored (the pair mode's second product)
+      double2 l[DOT == kDotLeft ? W : 1];
       if constexpr (MODE == kDotOnly) {
         ldw<W>(t1 + base, r2);
       } else {
@@ -1441,6 +1456,8 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_
               body(m);
           }
         }
+        if constexpr (DOT == kDotLeft && GQT_LEFT_EARLY)
+          ldw<W>(left + base, l);
         if constexpr (MODE == kCheb) {
           double2 y0[W];
           ldw<W>(t0 + base, y0);
@@ -1456,8 +1473,8 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_
         stw<W>(out + base, r2);
       }
       if constexpr (DOT == kDotLeft) {
-        double2 l[W];
-        ldw<W>(left + base, l);
+        if constexpr (MODE == kDotOnly || !GQT_LEFT_EARLY)
+          ldw<W>(left + base, l);
 #pragma unroll
         for (int k = 0; k < W; ++k) {
           if constexpr (kExact) {

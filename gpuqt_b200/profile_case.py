@@ -7,8 +7,10 @@ one arithmetic form: fp64 (plain, one vector), fp32v1, or fp32vV (V vectors per
 launch, FP32 storage), with the operator in the coded format (the default where the
 lattice has one) or in the plain ELL arrays (`--format ell`). With `--doubled` each
 set is a symmetric moment set from half the Chebyshev steps (gqt_moments_doubled: the
-step kernels in pair mode); the rate counts the moments produced. Prints one JSON line
-with the measured rate.
+step kernels in pair mode); the rate counts the moments produced. With `--evolve`
+each set is instead one evolve and one evolvex of the workload's first time step
+(the Bessel-series kernels k_cheb2 and k_cheb2x), timed separately. Prints one JSON
+line with the measured rate.
 """
 from __future__ import annotations
 
@@ -35,6 +37,8 @@ def main() -> None:
                     help="let the autotuner pick the shape for this vector count first")
     ap.add_argument("--doubled", action="store_true",
                     help="symmetric moment sets from half the steps (pair-mode kernels)")
+    ap.add_argument("--evolve", action="store_true",
+                    help="time evolve and evolvex of one time step instead of moments")
     args = ap.parse_args()
 
     import torch
@@ -74,6 +78,33 @@ def main() -> None:
         mu = torch.empty(2 * args.moments * V * R, dtype=torch.float64, device="cuda")
         stream = torch.cuda.current_stream()
         g.set_stream(stream.cuda_stream)
+        if args.evolve:
+            if args.workload == "batch":
+                raise SystemExit("--evolve needs a single model")
+            dt = float(m.time_step[0]) * m.energy_max
+            ev = lambda: (torch.cuda.Event(enable_timing=True),
+                          torch.cuda.Event(enable_timing=True))
+            g.evolve(H, 1, dt, X)
+            g.evolvex(H, 1, dt, X)
+            before = g.launch_count()
+            a, b = ev()
+            a.record(stream)
+            for _ in range(args.sets):
+                g.evolve(H, 1, dt, X)
+            b.record(stream)
+            terms = (g.launch_count() - before) // args.sets - 2
+            c, d = ev()
+            c.record(stream)
+            for _ in range(args.sets):
+                g.evolvex(H, 1, dt, X)
+            d.record(stream)
+            torch.cuda.synchronize()
+            print(json.dumps({"workload": args.workload, "form": args.form, "sites": sites,
+                              "format": "coded" if H.format == g.FORMAT_CODED else "ell",
+                              "dt_scaled": dt, "bessel_terms": terms, "sets": args.sets,
+                              "ms_evolve": a.elapsed_time(b) / args.sets,
+                              "ms_evolvex": c.elapsed_time(d) / args.sets}))
+            return
         if args.doubled:
             def one():
                 g.moments_doubled_device(H, X, args.moments, mu.data_ptr())

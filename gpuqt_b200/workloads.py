@@ -101,6 +101,12 @@ CONFIGS = {
         kind="square", cells=(1024, 1024, 1), hopping=-1.0, anderson=2.0, energy_max=5.2,
         moments=2000, time_step=[1.0], calculate=(), seed=17,
         description="square 1024x1024 = 1,048,576 sites, z=4, t=-1, W=2 (seed 17), E_max 5.2"),
+    "cubic_slab": dict(
+        kind="cubic", cells=(32, 256, 256), hopping=-1.0, anderson=16.5, energy_max=15.0,
+        moments=4000, time_step=[1.0] * 30, calculate=("vac", "msd"), seed=13,
+        description="cubic slab 32x256x256 = 2,097,152 sites, z=6, the 65,536-site plane "
+                    "stride of 256^3 (a profiling size for it), t=-1, W=16.5 (seed 13), "
+                    "E_max 15"),
     "cubic256": dict(
         kind="cubic", cells=(256, 256, 256), hopping=-1.0, anderson=16.5, energy_max=15.0,
         moments=4000, time_step=[1.0] * 30, calculate=("vac", "msd"), seed=13,
