@@ -98,7 +98,9 @@ def test_fp32x_is_internal_to_the_moment_loop():
     with pytest.raises(g.GqtError):
         g.Vector(m.n, precision=g.FP32X)
     H = g.Hamiltonian(m)
-    x = g.Vector.from_host(*[np.stack([v] * 8) for v in m.initial_state()], nvec=8)
+    # FP32 has an 8-vector form, FP32X does not
+    x = g.Vector.from_host(*[np.stack([v] * 8) for v in m.initial_state()], nvec=8,
+                           precision=g.FP32)
     with pytest.raises(g.GqtError):  # no 8-vector FP32X launch
         g.moments(H, x, x, m.n_moments, precision=g.FP32X)
     B = g.Hamiltonian.batch([m, g.Model.load(fixture_dir("sq16_pbc"))])
