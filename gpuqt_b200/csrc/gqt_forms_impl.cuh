@@ -144,6 +144,11 @@ struct OpImpl {
           if (op.wpt == W2)
             return run(std::integral_constant<int, W2>{});
         }
+        if constexpr (std::is_same<VT2, xf2>::value && Z == 3 && V >= 4) {
+          // FP32X on rows of three: 4 vectors per thread fit the register budget there
+          // (rows of 4 and 6 spill at 4, hence 2 elsewhere)
+          return run(std::integral_constant<int, 4>{});
+        }
         return run(std::integral_constant<int, W>{});
       }
       // Programmatic dependent launch for the FP64 step (+1-2 % there; the FP32 step
