@@ -1397,31 +1397,49 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_
         ++r;
     }
     any = true;
-    // Software-pipelined within the tile: the next item's row is loaded first.
+    // Software-pipelined within the tile: the next item's row is loaded first, and in
+    // pair mode (kPreS) its streamed inputs too, as in k_step_vec.
     constexpr bool kPre = Z > 0 && pipelined<kPipeStepMulti, C, VT2, Z>() && MODE != kDotOnly;
+    // (rows of six spill with the look-ahead at this kernel's budget)
+    constexpr bool kPreS = kPre && vec_streams_ahead<VT2, DOT>() && Z < 6;
+    constexpr int kSM = MODE == kDotOnly ? kApply : MODE;  // VecStreams' mode
     RowIdx<(Z > 0 ? Z : 1)> cur, nxt;
+    VecStreams<VT2, W, kSM, DOT> sc;
     if constexpr (kPre) {
-      if (threadIdx.x < items_per_tile)
-        fetch_row<(Z > 0 ? Z : 1), C>(op, (int)(((size_t)t * items_per_tile + threadIdx.x) / kTps), cur);
+      if (threadIdx.x < items_per_tile) {
+        const size_t g0 = (size_t)t * items_per_tile + threadIdx.x;
+        fetch_row<(Z > 0 ? Z : 1), C>(op, (int)(g0 / kTps), cur);
+        if constexpr (kPreS)
+          fetch_vec_streams<V, W, kTps, kSM, DOT>(op, g0, t0, t1, left, sc);
+      }
     }
     for (size_t it = threadIdx.x; it < items_per_tile; it += kBlock) {
       const size_t g = (size_t)t * items_per_tile + it;
+      VecStreams<VT2, W, kSM, DOT> s;
+      if constexpr (kPreS)
+        s = sc;
       if constexpr (kPre) {
         nxt = cur;
-        if (it + kBlock < items_per_tile)
+        if (it + kBlock < items_per_tile) {
           fetch_row<(Z > 0 ? Z : 1), C>(op, (int)((g + kBlock) / kTps), nxt);
+          if constexpr (kPreS)
+            fetch_vec_streams<V, W, kTps, kSM, DOT>(op, g + kBlock, t0, t1, left, sc);
+        }
       }
       const int i = (int)(g / kTps);
       const int v0 = (int)(g % kTps) * W;
       const size_t base = (size_t)i * V + v0;
       double2 r2[W];
-      VT2 x[W];  // T_{k-1} as stored (the pair mode's second product)
       double2 l[DOT == kDotLeft ? W : 1];
+      if constexpr (!kPreS && MODE != kDotOnly) {
+        s.p = op.pot[i];
+        ldw_raw<W>(t1 + base, s.x);
+      }
+      const auto& x = s.x;  // T_{k-1} as stored (the pair mode's second product)
       if constexpr (MODE == kDotOnly) {
         ldw<W>(t1 + base, r2);
       } else {
-        const double p = op.pot[i];
-        ldw_raw<W>(t1 + base, x);
+        const double p = s.p;
         double tr[W], ti[W];
 #pragma unroll
         for (int k = 0; k < W; ++k) {
@@ -1459,12 +1477,14 @@ __global__ void __launch_bounds__(kBlock, multi_min_blocks<C, Z, DOT>()) k_step_
         if constexpr (DOT == kDotLeft && GQT_LEFT_EARLY)
           ldw<W>(left + base, l);
         if constexpr (MODE == kCheb) {
-          double2 y0[W];
-          ldw<W>(t0 + base, y0);
+          if constexpr (!kPreS)
+            ldw_raw<W>(t0 + base, s.y0);
 #pragma unroll
-          for (int k = 0; k < W; ++k)
-            r2[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0[k].x),
-                                 A::two_x_minus(A::scale(ti[k], op), y0[k].y));
+          for (int k = 0; k < W; ++k) {
+            const double2 y0 = widen(s.y0[k]);
+            r2[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0.x),
+                                 A::two_x_minus(A::scale(ti[k], op), y0.y));
+          }
         } else {
 #pragma unroll
           for (int k = 0; k < W; ++k)
