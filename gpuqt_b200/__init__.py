@@ -70,6 +70,8 @@ _SIGS = {
     "gqt_ham_format": (ctypes.c_int, [_vp, _ip, _ip]),
     "gqt_ham_set_batch_tile": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gqt_ham_batch_tile": (ctypes.c_int, [_vp, _ip]),
+    "gqt_ham_set_loop": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
+    "gqt_ham_loop": (ctypes.c_int, [_vp, _ip, _ip, _ip]),
     "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
                                             ctypes.POINTER(_vp)]),
     "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
@@ -382,6 +384,19 @@ class Hamiltonian:
 
     def set_batch_tile(self, tile_sites: int) -> None:
         _call("gqt_ham_set_batch_tile", self.h, int(tile_sites))
+
+    def set_loop(self, window: int, chunk_sites: int = 0) -> None:
+        """Moment loop of the FP64 form: 0 one launch per step, S >= 2 the wavefront
+        loop of S steps per launch over chunks of chunk_sites sites (0: 1024)
+        (gqt_ham_set_loop)."""
+        _call("gqt_ham_set_loop", self.h, int(window), int(chunk_sites))
+
+    @property
+    def loop(self) -> tuple[int, int, int]:
+        """(window, chunks, halo) of the moment loop (gqt_ham_loop)."""
+        w, c, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _call("gqt_ham_loop", self.h, ctypes.byref(w), ctypes.byref(c), ctypes.byref(k))
+        return w.value, c.value, k.value
 
     def set_format(self, fmt: int) -> None:
         """FORMAT_ELL or FORMAT_CODED (the default when the operator has a coded form)."""

@@ -1,6 +1,7 @@
 // Operator and algorithm entry points of the C ABI: apply / commutator / current,
 // the Chebyshev terms, the moment loop (find_moments_chebyshev), evolve, evolvex and
 // the Jackson-damped Chebyshev summation. See include/gpuqt.h.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -8,6 +9,7 @@
 #include "gqt_algo.h"
 #include "gqt_forms.h"
 #include "gqt_internal.h"
+#include "gqt_wave.cuh"
 
 namespace gqt {
 
@@ -25,6 +27,8 @@ Workspace::~Workspace()
   cudaFreeHost(mu_host);
   cudaFree(pairs);
   cudaFree(xarena);
+  cudaFree(wave_done);
+  cudaFree(wave_ctl);
   if (ev_in)
     cudaEventDestroy(ev_in);
   if (ev_out)
@@ -316,6 +320,157 @@ struct BatchDeferred {
   }
 };
 
+// ------------------------------------------------------------------ wavefront loop
+
+// Whether the wavefront loop applies to this moment loop (before planning).
+bool wave_eligible(const gqt_ham* h, const gqt_vec* right, bool pair)
+{
+  return h->loop_window >= 2 && !pair && h->n_real == 1 && right->precision == GQT_FP64 &&
+         right->nvec == 1 && h->use_codes && h->code &&
+         (h->z == 3 || h->z == 4 || h->z == 6);
+}
+
+// The chunk plan of the coded operator (entries j = i + delta): for every chunk, the
+// chunks its entries can reach, with each delta assumed at every site of the chunk
+// (j is always a site, so a reach is clipped to [0, n)). The halo is the largest
+// distance between a chunk and one it reaches, in positions of the identity order or
+// of the folded one (0, C-1, 1, C-2, ...: a periodic boundary joins chunks 0 and C-1),
+// whichever is smaller. Not applicable when the halo exceeds a quarter of the chunks.
+gqt_status wave_plan(const gqt_ham* h)
+{
+  h->wave_halo = -2;
+  const int n = h->n, cs = h->loop_chunk;
+  const int C = (n + cs - 1) / cs;
+  if (C < 16)
+    return GQT_OK;
+  std::vector<int> d(h->n_codes);
+  GQT_CUDA(cudaMemcpy(d.data(), h->code_delta, d.size() * sizeof(int), cudaMemcpyDeviceToHost));
+  std::sort(d.begin(), d.end());
+  d.erase(std::unique(d.begin(), d.end()), d.end());
+  int best = -1, best_fold = 0;
+  std::vector<int> pos(C);
+  for (int fold = 0; fold <= 1; ++fold) {
+    WavePlan wp{C, cs, 0, 1, fold};
+    for (int q = 0; q < C; ++q)
+      pos[wave_chunk(wp, q)] = q;
+    int K = 0;
+    for (int c = 0; c < C; ++c) {
+      const long long first = (long long)c * cs;
+      const long long last = std::min<long long>(first + cs, n) - 1;
+      for (int delta : d) {
+        long long lo = first + delta, hi = last + delta;
+        if (hi < 0 || lo > n - 1)
+          continue;
+        lo = std::max<long long>(lo, 0);
+        hi = std::min<long long>(hi, n - 1);
+        for (long long c2 = lo / cs; c2 <= hi / cs; ++c2)
+          K = std::max(K, std::abs(pos[c2] - pos[c]));
+      }
+    }
+    if (best < 0 || K < best) {
+      best = K;
+      best_fold = fold;
+    }
+  }
+  if (best > C / 4)
+    return GQT_OK;
+  h->wave_chunks = C;
+  h->wave_sites = cs;
+  h->wave_halo = best;
+  h->wave_fold = best_fold;
+  return GQT_OK;
+}
+
+// Plan (once) and size the workspace of a wavefront loop; outside any capture.
+gqt_status wave_prepare(const gqt_ham* h, Workspace& ws)
+{
+  if (h->wave_halo == -1)
+    GQT_TRY(wave_plan(h));
+  if (h->wave_halo < 0)
+    return GQT_OK;
+  if (ws.wave_done_n < h->wave_chunks) {
+    cudaStreamSynchronize(stream());
+    for (auto& kv : ws.graphs)
+      cudaGraphExecDestroy(kv.second);
+    ws.graphs.clear();
+    cudaFree(ws.wave_done);
+    ws.wave_done = nullptr;
+    ws.wave_done_n = 0;
+    GQT_CUDA(cudaMalloc(&ws.wave_done, (size_t)h->wave_chunks * sizeof(int)));
+    ws.wave_done_n = h->wave_chunks;
+  }
+  if (!ws.wave_ctl) {
+    GQT_CUDA(cudaMalloc(&ws.wave_ctl, 4 * sizeof(unsigned)));
+    GQT_CUDA(cudaMemset(ws.wave_ctl, 0, 4 * sizeof(unsigned)));
+  }
+  return GQT_OK;
+}
+
+// Doubles of the dot scratch a wavefront loop of window S needs: the immediate
+// partials, then S slab rows of chunks x warps partials.
+size_t wave_scratch(const gqt_ham* h)
+{
+  return (size_t)max_grid() * 32 * 4 +
+         (size_t)h->loop_window * h->wave_chunks * kWaveWarps * 4;
+}
+
+template <int Z>
+gqt_status wave_windows(const gqt_ham* h, const Op& op, const gqt_vec* left,
+                        const gqt_vec* right, int M, double2* mu, void* A, void* B,
+                        DotScratch* ds, Workspace& ws)
+{
+  cudaStream_t s = stream();
+  const int S = h->loop_window;
+  const int G = grid_for((const void*)k_wave<Z>, (size_t)1 << 40);
+  // lag: the halo plus about one round of the resident blocks' tickets, so an item's
+  // dependencies were handed out a round earlier
+  WavePlan wp{h->wave_chunks, h->wave_sites, h->wave_halo,
+              h->wave_halo + (G + S - 1) / S + 2, h->wave_fold};
+  WaveCtl* ctl = reinterpret_cast<WaveCtl*>(ws.wave_ctl);
+  k_wave_init<<<(wp.chunks + kBlock - 1) / kBlock, kBlock, 0, s>>>(
+    ws.wave_done, wp.chunks, ctl, ds->counter, (unsigned)(wp.chunks * kWaveWarps));
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  double* slab = ds->partials + (size_t)max_grid() * 32 * 4;
+  const size_t row = (size_t)wp.chunks * kWaveWarps * 4;
+  for (int s0 = 2; s0 < M; s0 += S) {
+    const int steps = std::min(S, M - s0);
+    k_wave<Z><<<G, kBlock, op_smem_bytes(op), s>>>(
+      op, wp, s0, steps, (const double2*)right->data, (double2*)A, (double2*)B,
+      (const double2*)left->data, ws.wave_done, ctl, slab);
+    k_slab_combine<1><<<steps, kBlock, 0, s>>>(slab, row, ds->counter, mu + s0);
+    count_launches(2);
+    GQT_CUDA(cudaGetLastError());
+  }
+  return GQT_OK;
+}
+
+// The moment loop with steps 2 .. M-1 as wavefront windows (moments 0 and 1 as in the
+// step loop).
+gqt_status wave_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* left,
+                         const gqt_vec* right, int M, double2* mu, void* A, void* B,
+                         DotScratch* ds)
+{
+  Op op = make_op(h, 1);
+  Dot d{ds->partials, ds->counter, mu};
+  GQT_TRY(f->dot((size_t)h->n, right->data, left->data, d));
+  if (M < 2)
+    return GQT_OK;
+  d.mu = mu + 1;
+  GQT_TRY(f->step(op, kApply, nullptr, right->data, A, left->data, &d));
+  if (M < 3)
+    return GQT_OK;
+  Workspace& ws = *h->ws;
+  switch (h->z) {
+    case 3:
+      return wave_windows<3>(h, op, left, right, M, mu, A, B, ds, ws);
+    case 4:
+      return wave_windows<4>(h, op, left, right, M, mu, A, B, ds, ws);
+    default:
+      return wave_windows<6>(h, op, left, right, M, mu, A, B, ds, ws);
+  }
+}
+
 // The launch sequence of the moment loop (src/sigma.cu:33-61) on the current stream.
 // Buffers: T_0 = right (read only), T_1 -> A, then T_m overwrites T_{m-2} in place.
 gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* left,
@@ -348,6 +503,8 @@ gqt_status moment_launches(const gqt_ham* h, const FormOps* f, const gqt_vec* le
     }
     return GQT_OK;
   }
+  if (wave_eligible(h, right, false) && h->wave_halo >= 0)
+    return wave_launches(h, f, left, right, M, mu, A, B, ds);
   Dot d{ds->partials, ds->counter, mu, 0, right->xlo};
   GQT_TRY(f->dot(total, right->data, left->data, d));
   if (M < 2)
@@ -694,6 +851,11 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
   if (!mu_dev)
     return fail(GQT_ERR_ARG, "%s: null output", w);
   Workspace& ws = *h->ws;
+  if (wave_eligible(h, right, pair)) {
+    GQT_TRY(wave_prepare(h, ws));
+    if (h->wave_halo >= 0)
+      GQT_TRY(ws_dot(ws, wave_scratch(h), &ds));
+  }
   cudaStream_t s = stream();
   if (pair) {
     if (!h->hermitian)
@@ -930,6 +1092,17 @@ static gqt_status moments_host(const gqt_ham* h, const gqt_vec* left, const gqt_
   const double2* host = ws.mu_host;
   GQT_CUDA(cudaMemcpyAsync(ws.mu_host, ws.mu, need, cudaMemcpyDeviceToHost, stream()));
   GQT_CUDA(cudaStreamSynchronize(stream()));
+  if (ws.wave_ctl) {
+    // a wavefront loop whose bounded wait ran out flagged it (never expected: every
+    // wait is on an earlier ticket)
+    unsigned err = 0;
+    GQT_CUDA(cudaMemcpy(&err, ws.wave_ctl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (err) {
+      GQT_CUDA(cudaMemset(ws.wave_ctl + 2, 0, sizeof(unsigned)));
+      return fail(GQT_ERR_STATE, "%s: a wait of the wavefront loop timed out; moments invalid",
+                  w);
+    }
+  }
   for (int k = 0; k < V; ++k)
     for (int m = 0; m < M; ++m) {
       mu_re[(size_t)k * M + m] = host[(size_t)m * V + k].x;
@@ -1079,6 +1252,47 @@ extern "C" gqt_status gqt_chebyshev_summation(int M, double* mu_re, double* mu_i
     temp /= std::sqrt(1.0 - es * es);
     out[e] = temp / energy_max;
   }
+  return GQT_OK;
+}
+
+// ------------------------------------------------------------------ loop selection
+extern "C" gqt_status gqt_ham_set_loop(gqt_ham* h, int window, int chunk_sites)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_loop: null handle");
+  if (window != 0 && (window < 2 || window > 64))
+    return fail(GQT_ERR_ARG, "gqt_ham_set_loop: window must be 0 or 2..64 (got %d)", window);
+  if (chunk_sites == 0)
+    chunk_sites = 1024;
+  if (chunk_sites < kBlock || chunk_sites > (1 << 16) || chunk_sites % kBlock)
+    return fail(GQT_ERR_ARG,
+                "gqt_ham_set_loop: chunk_sites must be a multiple of %d up to 65536 (got %d)",
+                kBlock, chunk_sites);
+  if (chunk_sites != h->loop_chunk) {
+    h->loop_chunk = chunk_sites;
+    h->wave_halo = -1;  // plan again
+  }
+  if (h->ws) {
+    // Graphs captured so far launch the other loop.
+    cudaStreamSynchronize(stream());
+    for (auto& kv : h->ws->graphs)
+      cudaGraphExecDestroy(kv.second);
+    h->ws->graphs.clear();
+  }
+  h->loop_window = window;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_loop: null handle");
+  if (window)
+    *window = h->loop_window;
+  if (chunks)
+    *chunks = h->wave_halo >= 0 ? h->wave_chunks : 0;
+  if (halo)
+    *halo = h->wave_halo;
   return GQT_OK;
 }
 

@@ -34,6 +34,11 @@ struct Workspace {
   unsigned char* xarena = nullptr;
   size_t xslot = 0;
   uintptr_t xlo = 0;
+  // Wavefront moment loop: the last step done per chunk position, and its counters
+  // (ticket, exited, error, pad).
+  int* wave_done = nullptr;
+  int wave_done_n = 0;
+  unsigned* wave_ctl = nullptr;
   // Instantiated moment loops: (left, right, n_moments, mu, precision, nvec, loop),
   // loop 0 the direct one, 1 the symmetric (pair) one.
   using GraphKey = std::tuple<const void*, const void*, int, void*, int, int, int>;

@@ -107,6 +107,13 @@ struct gqt_ham {
   // Vectors per thread of the batched step for each vector count (0: the form's
   // default); set by the autotuner.
   mutable int wpt[33] = {};
+  // Moment loop of the FP64 form: 0 one launch per step; S >= 2 the wavefront loop,
+  // S steps per launch (gqt_ham_set_loop). Its plan, made on first use: chunks of
+  // wave_sites sites, the halo in positions (-1 not planned yet, -2 not applicable)
+  // and the position order (1: folded).
+  int loop_window = 0;
+  int loop_chunk = 1024;  // sites per chunk of the wavefront loop
+  mutable int wave_chunks = 0, wave_sites = 0, wave_halo = -1, wave_fold = 0;
   std::unique_ptr<gqt::Workspace> ws;
   ~gqt_ham();
 };

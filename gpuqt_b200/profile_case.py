@@ -39,6 +39,10 @@ def main() -> None:
                     help="symmetric moment sets from half the steps (pair-mode kernels)")
     ap.add_argument("--evolve", action="store_true",
                     help="time evolve and evolvex of one time step instead of moments")
+    ap.add_argument("--loop", type=int, default=0,
+                    help="FP64 moment loop: 0 step by step, S >= 2 wavefront windows of S")
+    ap.add_argument("--chunk", type=int, default=0,
+                    help="sites per chunk of the wavefront loop (0: the default)")
     args = ap.parse_args()
 
     import torch
@@ -71,6 +75,8 @@ def main() -> None:
             sites = m.n
         if args.format != "default":
             H.set_format(g.FORMAT_ELL if args.format == "ell" else g.FORMAT_CODED)
+        if args.loop:
+            H.set_loop(args.loop, args.chunk)
         tuned = None
         if args.autotune:
             tuned = g.autotune_nvec(H, prec, 20, [V])[1]
@@ -124,7 +130,7 @@ def main() -> None:
                           "format": "coded" if H.format == g.FORMAT_CODED else "ell",
                           "n_codes": H.n_codes,
                           "moments": args.moments, "sets": args.sets, "autotune": tuned,
-                          "doubled": args.doubled,
+                          "doubled": args.doubled, "loop": list(H.loop),
                           "site_moments_per_s": V * sites * args.moments * args.sets / s}))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

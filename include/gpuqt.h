@@ -130,6 +130,23 @@ gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count, gqt_ham** 
  * between tile sizes to rounding (the per-block sums group differently). */
 gqt_status gqt_ham_set_batch_tile(gqt_ham* h, int tile_sites);
 gqt_status gqt_ham_batch_tile(const gqt_ham* h, int* tile_sites);
+
+/* The moment loop of the FP64 form (no counterpart in the reference, which launches
+ * one step at a time). window 0: one launch per Chebyshev step (the default). window
+ * S >= 2: the wavefront loop, S steps per persistent launch. The sites are cut into
+ * chunks; each block takes (step, chunk) items from a ticket counter in an order in
+ * which every item depends only on earlier tickets, and starts one as soon as the
+ * previous step is done on the chunks its rows reach. So the S steps run as a wave
+ * through L2 and only the leading step reads its vectors from HBM. It applies to one
+ * model, one FP64 vector, the coded operator, rows of 3, 4 or 6 entries, and a halo
+ * small against the lattice. Other loops run step by step. Every T_m is bit-identical
+ * between the two loops; the moments are summed in another fixed order (equal to
+ * 1e-12). chunk_sites (a multiple of 256; 0: 1024) sets the chunk: smaller chunks
+ * shorten the distance at which the next step reuses a chunk's data, larger ones
+ * spend less on each item's hand-over. gqt_ham_loop reports the window and, once a loop has run, the plan (chunks
+ * and halo in chunk positions; halo -2: not applicable). */
+gqt_status gqt_ham_set_loop(gqt_ham* h, int window, int chunk_sites);
+gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo);
 gqt_status gqt_ham_realisations(const gqt_ham* h, int* count);
 gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
                                double* energy_max);
