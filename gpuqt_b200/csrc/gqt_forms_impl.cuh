@@ -78,11 +78,6 @@ gqt_status launch_smem(K* kernel, size_t total, size_t smem, Args... args)
   return GQT_OK;
 }
 
-// FP32-element vectors per thread in pair mode (2; a build may set 4 for timing).
-#ifndef GQT_PAIR_W_FP32
-#define GQT_PAIR_W_FP32 2
-#endif
-
 // Storage types with FP32 elements (float2; xf2, FP32 with a BF16 residual).
 template <typename VT2>
 struct Fp32Like
@@ -106,12 +101,15 @@ struct OpImpl {
   // vectors per thread: half the accumulator registers, twice the threads per site).
   static constexpr int W = vectors_per_thread<VT2, V>();
   static constexpr int W2 = (std::is_same<VT2, float2>::value && V >= 4) ? 2 : W;
-  // Vectors a thread advances in the pair mode of a symmetric moment set: 2 float2 or 1
-  // double2. The pair mode keeps three FP64 sums per vector and T_{k-1} until the end
-  // of an item; at the direct step's width (4 float2, 2 double2) that spilled 120-250
-  // bytes per thread at the step's register budget.
-  static constexpr int WP =
-    Fp32Like<VT2>::value ? (V < GQT_PAIR_W_FP32 ? V : GQT_PAIR_W_FP32) : 1;
+  // Vectors a thread advances in the pair mode of a symmetric moment set. The pair mode
+  // keeps three FP64 sums per vector and T_{k-1} until the end of an item. k_step_vec:
+  // 4 float2 with 128 registers (2 blocks per SM; 13.6 % faster on B200 than 2 float2
+  // at 85 registers), 2 FP32X elements, 1 double2. k_step_multi (80 registers): 2
+  // FP32-element vectors, 1 double2.
+  static constexpr int WP = std::is_same<VT2, float2>::value
+                              ? (V < 4 ? V : 4)
+                              : (std::is_same<VT2, xf2>::value ? (V < 2 ? V : 2) : 1);
+  static constexpr int WPM = Fp32Like<VT2>::value ? (V < 2 ? V : 2) : 1;
 
   static gqt_status step(const Op& op, int mode, const void* t0, const void* t1, void* out,
                          const void* left, const Dot* dot)
@@ -222,8 +220,8 @@ struct OpImpl {
       };
       if (dot == kDotPair && mode != kDotOnly) {
         if (mode == kApply)
-          return go(k_step_multi<VT2, V, WP, Z, A, kApply, C, kDotPair>);
-        return go(k_step_multi<VT2, V, WP, Z, A, kCheb, C, kDotPair>);
+          return go(k_step_multi<VT2, V, WPM, Z, A, kApply, C, kDotPair>);
+        return go(k_step_multi<VT2, V, WPM, Z, A, kCheb, C, kDotPair>);
       }
       auto pick = [&](auto wc) -> gqt_status {
         constexpr int WW = decltype(wc)::value;

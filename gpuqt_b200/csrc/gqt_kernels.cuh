@@ -1097,11 +1097,6 @@ __device__ __forceinline__ void fetch_vec_streams(const Op& op, size_t g, const 
 #ifndef GQT_LEFT_EARLY
 #define GQT_LEFT_EARLY 0
 #endif
-// Blocks per SM of the pair-mode step on rows of known length (0: the defaults below; a
-// build may set it for timing).
-#ifndef GQT_PAIR_MINB
-#define GQT_PAIR_MINB 0
-#endif
 template <typename VT2, int DOT>
 __host__ __device__ constexpr bool vec_streams_ahead()
 {
@@ -1111,9 +1106,11 @@ __host__ __device__ constexpr bool vec_streams_ahead()
 }
 
 // The pair mode of a symmetric set keeps three sums per vector and T_{k-1} for the whole
-// item: rows of unknown length (Z = 0), and the FP64 and FP32X forms on rows of six,
-// take 3 blocks per SM there (at 4 they spilled 16-140 bytes per thread), the FP64
-// form on rows of unknown length 2 (12-24 bytes at 3).
+// item. The FP32 form advances 4 vectors per thread there with its streamed inputs one
+// item ahead: 2 blocks per SM (128 registers). The FP64 form, with the look-ahead,
+// takes 3 blocks (2 on rows of unknown length: 12-24 bytes of spills at 3); the FP32X
+// form, without it, 3 on rows of six and of unknown length (at 4 they spilled 16-140
+// bytes per thread) and 4 otherwise.
 constexpr int kVecMinBlocks = 4;
 template <typename VT2, int Z, int DOT>
 constexpr int vec_min_blocks()
@@ -1121,12 +1118,14 @@ constexpr int vec_min_blocks()
   constexpr bool f64 = std::is_same<VT2, double2>::value;
   if constexpr (DOT != kDotPair)
     return kVecMinBlocks;
-  else if constexpr ((vec_streams_ahead<VT2, DOT>() || GQT_PAIR_MINB > 0) && Z > 0)
-    return GQT_PAIR_MINB > 0 ? GQT_PAIR_MINB : 3;  // the look-ahead's second set of streams
+  else if constexpr (std::is_same<VT2, float2>::value)
+    return 2;
   else if constexpr (Z <= 0)
     return f64 ? 2 : 3;
+  else if constexpr (vec_streams_ahead<VT2, DOT>())
+    return 3;  // FP64: the look-ahead's second set of streams
   else
-    return (Z >= 6 && !std::is_same<VT2, float2>::value) ? 3 : kVecMinBlocks;
+    return Z >= 6 ? 3 : kVecMinBlocks;
 }
 template <bool C, int Z = 4, int DOT = kDotLeft>
 constexpr int multi_min_blocks()
