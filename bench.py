@@ -244,6 +244,28 @@ def time_reference(ref_dir, n_moments, reps, procs):
     return [max(p[r] for p in per) for r in range(reps)], None
 
 
+def cpu_baseline_configs(tmp, names=("graphene4m", "cubic256"), n_moments_sample=16,
+                         reps=2):
+    """The reference's CPU moment loop on the larger workloads (one process: its 1-core
+    rate), a bounded sample of moments each; the rate per site-moment does not depend
+    on the count."""
+    from gpuqt_b200 import workloads as W
+    out = {}
+    for name in names:
+        rd = reference_dir(W.config_dir(os.path.join(tmp, "cpu"), name),
+                           os.path.join(tmp, "cpu_ref", name))
+        t, why = time_reference(rd, n_moments_sample, reps, 1)
+        if t is None:
+            out[name] = {"value_1_core": None, "why": why}
+            continue
+        out[name] = {"value_1_core": W.config_sites(name) * n_moments_sample /
+                                     statistics.mean(t),
+                     "unit": UNIT, "sample": f"{n_moments_sample} moments per call, {reps} "
+                                             f"calls, one process, the reference's fixed "
+                                             f"seed"}
+    return out
+
+
 def cpu_baseline_line(ref_dir, n_sites, n_moments_sample=64, reps=3):
     """The reference's CPU moment loop on this host: one process (the reference is
     serial: its 1-core rate) and one process per core at once (the host's aggregate,
@@ -431,6 +453,8 @@ def run_ours(args):
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_line(reference_dir(src, os.path.join(tmp, "ref")), n)
+            if cpu.get("value") is not None:
+                cpu["other_workloads"] = cpu_baseline_configs(tmp)
 
         if rank == 0:
             line = {
