@@ -84,3 +84,34 @@ def test_autotuner_picks_a_candidate():
     assert best in (4, 8, 16, 32)
     assert all(v > 0 for v in rates.values())
     assert rates[best] == max(rates.values())
+
+
+@pytest.mark.parametrize("tile", [256, 512, 1024])
+def test_batch_tile_sizes_give_the_same_moments(tile):
+    """Every tile size the step can run with (the autotuner's choice) gives each model
+    the moments of the model run alone, the deferred window reductions included
+    (M = 120 > one window), in the direct and the symmetric (pair) loop."""
+    models = _models()
+    B = g.Hamiltonian.batch(models)
+    assert B.n % 1024 == 0 and B.batch_tile == 256
+    B.set_batch_tile(tile)
+    assert B.batch_tile == tile
+    ph = _phases(models, 4)
+    X = g.Vector.from_host(*B.scatter(ph), nvec=4)
+    M = 120
+    re, im = g.moments(B, X, X, M)
+    dr, di = g.moments_doubled(B, X, M)
+    for r, m in enumerate(models):
+        H = g.Hamiltonian(m)
+        for v in (0, 3):
+            x = g.Vector.from_host(ph[r][0][v], ph[r][1][v])
+            ref = g.moments(H, x, x, M)
+            assert _rel((re[r, v], im[r, v]), ref) <= 1e-12
+            assert np.max(np.hypot(dr[r, v] - ref[0], di[r, v] - ref[1])) <= (
+                1e-12 * np.max(np.hypot(*ref)))
+    with pytest.raises(g.GqtError):
+        B.set_batch_tile(384)
+    single = g.Hamiltonian(models[0])
+    assert single.batch_tile == 0
+    with pytest.raises(g.GqtError):
+        single.set_batch_tile(256)
