@@ -72,6 +72,8 @@ _SIGS = {
     "gqt_ham_batch_tile": (ctypes.c_int, [_vp, _ip]),
     "gqt_ham_set_loop": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int]),
     "gqt_ham_loop": (ctypes.c_int, [_vp, _ip, _ip, _ip]),
+    "gqt_ham_set_staging": (ctypes.c_int, [_vp, ctypes.c_int]),
+    "gqt_ham_staging": (ctypes.c_int, [_vp, _ip, _ip, _ip, _ip]),
     "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
                                             ctypes.POINTER(_vp)]),
     "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
@@ -397,6 +399,20 @@ class Hamiltonian:
         w, c, k = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         _call("gqt_ham_loop", self.h, ctypes.byref(w), ctypes.byref(c), ctypes.byref(k))
         return w.value, c.value, k.value
+
+    def set_staging(self, stages: int) -> None:
+        """Staged step of the FP32 moment loops: -1 off; 0 automatic (the default: the
+        symmetric loop is staged, the direct loop is not); 1 both loops, as many
+        shared-memory stages as fit; 2..4 both loops, that many (gqt_ham_set_staging)."""
+        _call("gqt_ham_set_staging", self.h, int(stages))
+
+    @property
+    def staging(self) -> tuple[int, list[tuple[int, int]]]:
+        """(stages setting, [(lo, hi) neighbour-offset window, ...]) (gqt_ham_staging)."""
+        s, nw = ctypes.c_int(), ctypes.c_int()
+        lo, hi = (ctypes.c_int * 8)(), (ctypes.c_int * 8)()
+        _call("gqt_ham_staging", self.h, ctypes.byref(s), ctypes.byref(nw), lo, hi)
+        return s.value, [(lo[w], hi[w]) for w in range(nw.value)]
 
     def set_format(self, fmt: int) -> None:
         """FORMAT_ELL or FORMAT_CODED (the default when the operator has a coded form)."""

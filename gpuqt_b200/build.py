@@ -29,7 +29,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["gqt_runtime.cu", "gqt_algo.cu", "gqt_forms_fp64.cu", "gqt_forms_fp32.cu",
               "gqt_forms_fp32x.cu",
-              "gqt_forms_fp64_coded.cu", "gqt_forms_fp32_coded.cu", "gqt_noalloc.cu"]
+              "gqt_forms_fp64_coded.cu", "gqt_forms_fp32_coded.cu", "gqt_noalloc.cu",
+              "gqt_stage.cu"]
 CPP_SOURCES = ["host/model.cpp", "host/vector_ham.cpp", "host/sigma.cpp", "host/lsqt.cpp",
                "host/checkpoint.cpp", "host/batch_run.cpp"]
 

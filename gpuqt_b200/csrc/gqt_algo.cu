@@ -138,6 +138,15 @@ Op make_op(const gqt_ham* h, int nvec = 1)
   op.emax = h->energy_max;
   op.inv_emax = 1.0 / h->energy_max;
   op.lib_div = !(h->energy_max >= 0x1p-100 && h->energy_max <= 0x1p100);
+  if (h->use_codes && h->n_real == 1 && h->stage_nw > 0 && h->stage_err) {
+    op.stage_nw = h->stage_nw;
+    op.stage_stages = h->stage_stages;
+    for (int w = 0; w < h->stage_nw; ++w) {
+      op.stage_lo[w] = h->stage_lo[w];
+      op.stage_hi[w] = h->stage_hi[w];
+    }
+    op.stage_err = h->stage_err;
+  }
   return op;
 }
 
@@ -1103,6 +1112,15 @@ static gqt_status moments_host(const gqt_ham* h, const gqt_vec* left, const gqt_
                   w);
     }
   }
+  if (h->stage_err) {
+    // a staged step whose bounded wait for its shared-memory copies ran out flagged it
+    unsigned err = 0;
+    GQT_CUDA(cudaMemcpy(&err, h->stage_err, sizeof(unsigned), cudaMemcpyDeviceToHost));
+    if (err) {
+      GQT_CUDA(cudaMemset(h->stage_err, 0, sizeof(unsigned)));
+      return fail(GQT_ERR_STATE, "%s: a wait of the staged step timed out; moments invalid", w);
+    }
+  }
   for (int k = 0; k < V; ++k)
     for (int m = 0; m < M; ++m) {
       mu_re[(size_t)k * M + m] = host[(size_t)m * V + k].x;
@@ -1293,6 +1311,41 @@ extern "C" gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, i
     *chunks = h->wave_halo >= 0 ? h->wave_chunks : 0;
   if (halo)
     *halo = h->wave_halo;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_set_staging(gqt_ham* h, int stages)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_staging: null handle");
+  if (stages < -1 || stages > 4)
+    return fail(GQT_ERR_ARG, "gqt_ham_set_staging: stages must be -1..4 (got %d)", stages);
+  if (h->ws) {
+    // Graphs captured so far launch the other step.
+    cudaStreamSynchronize(stream());
+    for (auto& kv : h->ws->graphs)
+      cudaGraphExecDestroy(kv.second);
+    h->ws->graphs.clear();
+  }
+  h->stage_stages = stages;
+  return GQT_OK;
+}
+
+extern "C" gqt_status gqt_ham_staging(const gqt_ham* h, int* stages, int* windows,
+                                      int* lo, int* hi)
+{
+  if (!h)
+    return fail(GQT_ERR_ARG, "gqt_ham_staging: null handle");
+  if (stages)
+    *stages = h->stage_stages;
+  if (windows)
+    *windows = h->use_codes ? h->stage_nw : 0;
+  for (int w = 0; w < h->stage_nw; ++w) {
+    if (lo)
+      lo[w] = h->stage_lo[w];
+    if (hi)
+      hi[w] = h->stage_hi[w];
+  }
   return GQT_OK;
 }
 

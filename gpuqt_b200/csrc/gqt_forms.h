@@ -111,6 +111,14 @@ inline const FormOps* form_ops(int precision, int nvec)
   return nullptr;
 }
 
+// The staged step of the FP32 moment loops over the coded operator (gqt_stage.cu): whether
+// it serves this step (op has staging windows, nvec 16 or 32, rows of 3, 4 or 6, dot kDotLeft
+// or kDotPair, 16-byte aligned vectors), and the step itself.
+bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
+                   const void* left);
+gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
+                      const void* t1, void* out, const void* left, const Dot& d);
+
 // Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
 // at the number of blocks that are resident at once on all SMs.
 int grid_for(const void* kernel, size_t total);

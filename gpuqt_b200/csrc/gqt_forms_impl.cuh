@@ -120,6 +120,10 @@ struct OpImpl {
     VT2* o = (VT2*)out;
     const VT2* l = (const VT2*)left;
     Dot d = dot ? *dot : Dot{nullptr, nullptr, nullptr};
+    if constexpr (C && std::is_same<VT2, float2>::value) {
+      if (dot && stage_applies(op, V, mode, kDotLeft, t0, t1, left))
+        return stage_step(op, V, mode, kDotLeft, t0, t1, out, left, d);
+    }
     return with_z(op.z, [&](auto zc) -> gqt_status {
       constexpr int Z = decltype(zc)::value;
       if constexpr (W > 1) {
@@ -177,6 +181,10 @@ struct OpImpl {
       const VT2* a0 = (const VT2*)t0;
       const VT2* a1 = (const VT2*)t1;
       VT2* o = (VT2*)out;
+      if constexpr (C && std::is_same<VT2, float2>::value) {
+        if (stage_applies(op, V, mode, kDotPair, t0, t1, nullptr))
+          return stage_step(op, V, mode, kDotPair, t0, t1, out, nullptr, d);
+      }
       return with_z(op.z, [&](auto zc) -> gqt_status {
         constexpr int Z = decltype(zc)::value;
         if constexpr (V > 1) {

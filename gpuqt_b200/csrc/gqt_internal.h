@@ -114,6 +114,14 @@ struct gqt_ham {
   int loop_window = 0;
   int loop_chunk = 1024;  // sites per chunk of the wavefront loop
   mutable int wave_chunks = 0, wave_sites = 0, wave_halo = -1, wave_fold = 0;
+  // Staged step of the FP32 moment loops (coded operator, gqt_ham_set_staging): the
+  // windows of frequent neighbour offsets [stage_lo[w], stage_hi[w]] (window 0 holds 0),
+  // the setting (-1 off; 0 automatic, the default: the symmetric loop is staged; 1 as
+  // many stages as fit; 2..4 that many) and the device flag a wait that ran out sets.
+  int stage_nw = 0;
+  int stage_lo[8] = {}, stage_hi[8] = {};
+  int stage_stages = 0;
+  unsigned* stage_err = nullptr;
   std::unique_ptr<gqt::Workspace> ws;
   ~gqt_ham();
 };

@@ -30,6 +30,8 @@
 namespace gqt {
 
 constexpr int kBlock = 256;
+// Windows of T_{k-1} rows the staged step (gqt_stage.cu) copies into shared memory per tile.
+constexpr int kStageWin = 8;
 
 struct Op {
   int n;
@@ -52,6 +54,14 @@ struct Op {
   const double* __restrict__ code_xx;
   int n_codes;
   uintptr_t xlo;  // FP32X storage: residual of the element at p is at xlo + p / 2
+  // Staged step of the FP32 moment loops over the coded operator (0 windows: not
+  // staged): window w covers the neighbour offsets j - i in [stage_lo[w], stage_hi[w]],
+  // window 0 holds offset 0; a wait that runs out sets *stage_err.
+  int stage_nw;
+  int stage_stages;  // -1 off; 0 automatic; 1 as many stages as fit; 2..4 stages
+  int stage_lo[kStageWin];
+  int stage_hi[kStageWin];
+  unsigned* stage_err;
 };
 
 struct Dot {
@@ -375,12 +385,20 @@ __device__ __forceinline__ void grid_combine(const double* partials, int nblocks
   }
 }
 
+// Vector of slot k of the threads with lane % (V / W) == q: the W consecutive vectors
+// q W .. q W + W - 1.
+struct ContigSlots {
+  __device__ __forceinline__ int operator()(int q, int k, int w) const { return q * w + k; }
+};
+
 // Combine per-thread partials across the block, then across the grid (last block,
 // fixed order, or k_slab_combine later when dot.defer is set), and write dot.mu[v] for
-// v < V. A thread holds the sums of W consecutive vectors v0 .. v0+W-1,
-// v0 = (lane % (V/W)) * W. Must be reached by every thread of the block.
-template <int V, int W>
-__device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const Dot& dot)
+// v < V. Slot k of a thread holds the sums of vector map(q, k, W), q = lane % (V/W)
+// (by default W consecutive vectors from q W). Must be reached by every thread of the
+// block.
+template <int V, int W, class Map = ContigSlots>
+__device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const Dot& dot,
+                                             Map map = Map{})
 {
   static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two <= 32");
   static_assert(W >= 1 && W <= V && V % W == 0, "W must divide V");
@@ -401,10 +419,11 @@ __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const
   if (lane < kTps) {
 #pragma unroll
     for (int k = 0; k < W; ++k) {
-      sh[warp][lane * W + k][0] = re[k].s;
-      sh[warp][lane * W + k][1] = re[k].c;
-      sh[warp][lane * W + k][2] = im[k].s;
-      sh[warp][lane * W + k][3] = im[k].c;
+      const int v = map(lane, k, W);
+      sh[warp][v][0] = re[k].s;
+      sh[warp][v][1] = re[k].c;
+      sh[warp][v][2] = im[k].s;
+      sh[warp][v][3] = im[k].c;
     }
   }
   __syncthreads();

@@ -440,6 +440,7 @@ gqt_ham::~gqt_ham()
   cudaFree(code_delta);
   cudaFree(code_hop);
   cudaFree(code_xx);
+  cudaFree(stage_err);
 }
 
 namespace {
@@ -699,6 +700,62 @@ bool is_hermitian(const Packed& P)
   return !broken;
 }
 
+// Windows of the staged FP32 step (gqt_stage.cu): the neighbour offsets j - i taken by
+// at least n / 64 entries, and offset 0, grouped where consecutive offsets lie at most
+// 16 rows apart; the group holding 0 first, then the most used, at most 8 in all. A
+// tile of the step copies each window's rows into shared memory; entries whose offset
+// lies in no window (periodic wraps, taken by a few rows per lattice line) gather from
+// global memory.
+void plan_stage_windows(const Packed& P, const std::vector<uint8_t>& codes,
+                        const std::vector<int>& delta, gqt_ham* h)
+{
+  static_assert(sizeof(h->stage_lo) / sizeof(int) == kStageWin, "window table size");
+  const size_t nc = delta.size();
+  std::vector<std::vector<long long>> part(16, std::vector<long long>(nc, 0));
+  parallel_rows(P.n, [&](long long lo, long long hi, int chunk) {
+    auto& u = part[chunk];
+    for (int m = 0; m < P.z; ++m)
+      for (long long i = lo; i < hi; ++i)
+        ++u[codes[(size_t)m * P.n + i]];
+  });
+  std::map<int, long long> use;  // offset -> entries
+  use[0] += 0;
+  for (size_t c = 0; c < nc; ++c) {
+    long long u = 0;
+    for (auto& p : part)
+      u += p[c];
+    use[delta[c]] += u;
+  }
+  struct Win {
+    int lo, hi;
+    long long use;
+  };
+  std::vector<Win> wins;
+  for (const auto& [d, u] : use) {
+    if (d != 0 && u < (long long)P.n / 64)
+      continue;
+    if (!wins.empty() && (long long)d - wins.back().hi <= 16) {
+      wins.back().hi = d;
+      wins.back().use += u;
+    } else {
+      wins.push_back(Win{d, d, u});
+    }
+  }
+  std::stable_sort(wins.begin(), wins.end(), [](const Win& a, const Win& b) {
+    const bool za = a.lo <= 0 && a.hi >= 0, zb = b.lo <= 0 && b.hi >= 0;
+    if (za != zb)
+      return za;
+    return a.use > b.use;
+  });
+  if (wins.size() > (size_t)kStageWin)
+    wins.resize(kStageWin);
+  h->stage_nw = (int)wins.size();
+  for (size_t w = 0; w < wins.size(); ++w) {
+    h->stage_lo[w] = wins[w].lo;
+    h->stage_hi[w] = wins[w].hi;
+  }
+}
+
 gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
 {
   const size_t pairs = (size_t)P.n * P.z;
@@ -737,6 +794,9 @@ gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ha
     GQT_CUDA(cudaMemcpy(h->code_xx, cxx.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
     h->n_codes = (int)nc;
     h->use_codes = 1;
+    plan_stage_windows(P, codes, delta, h);
+    GQT_CUDA(cudaMalloc(&h->stage_err, sizeof(unsigned)));
+    GQT_CUDA(cudaMemset(h->stage_err, 0, sizeof(unsigned)));
   }
   h->hermitian = is_hermitian(P) ? 1 : 0;
   h->ws.reset(new_workspace());

@@ -1,0 +1,513 @@
+// The staged Chebyshev step of the FP32 moment loops over the coded operator (sm_100a).
+//
+// The sites are cut into tiles of TS consecutive sites; block b takes tiles b, b + G,
+// b + 2G, ... (G resident blocks), so the GPU sweeps one compact front of tiles and the
+// rows a tile gathers were read by nearby tiles shortly before (L2 hits). A gather of
+// site i reads T_{k-1} at i + d for the offset d of its code. The frequent offsets form
+// a few windows: window w covers the offsets [lo_w, hi_w], so a tile starting at site t
+// reads the rows [t + lo_w, t + TS + hi_w) of it. With the vectors interleaved per site
+// ([site][vector]), each window is one contiguous byte range of T_{k-1}.
+//
+// Thread 0 copies a tile's windows, its T_{k-2} rows and (moment <left|T_k>) its left
+// rows into one of S shared-memory stages with bulk asynchronous copies (cp.async.bulk,
+// completing on the stage's mbarrier), S - 1 tiles ahead of the tile being computed.
+// The compute threads then read every vector operand from shared memory (one 16-byte
+// load per row and thread, conflict-free), so they wait on no global vector load; the
+// codes and the potential of the next tile are loaded one tile ahead into registers.
+// Offsets outside the windows (the periodic wraps: a few rows per lattice line) are
+// gathered from global memory.
+//
+// Per element the arithmetic is that of k_step_vec with FastArith (src/sigma.cu:33-61's
+// recurrence, the operator in FP64, T_k rounded to FP32 once), so T_k is the unstaged
+// step's bit for bit: entries past a row's length are the padding entries of the coded
+// table (offset 0, hopping 0) and add an exact zero instead of being skipped. The
+// moments are the same per-thread FP64 sums taken over the sites in another order.
+//
+// Every wait on an mbarrier is bounded; one that runs out sets *op.stage_err, stops the
+// block's further copies and is waited for once more (bounded) before the block exits.
+#include "gqt_forms.h"
+
+#include <mutex>
+#include <unordered_map>
+
+namespace gqt {
+
+namespace {
+
+constexpr int kMaxStages = 4;
+constexpr int kStageW = 4;  // vectors per thread: two 16-byte chunks of a row
+
+// Byte layout of one stage for a launch (host-computed from the operator's windows).
+struct StageLayout {
+  int stages;
+  int stage_bytes;
+  int nw;
+  int win_lo[kStageWin];    // window w holds rows [tile + win_lo, tile + win_lo + win_rows)
+  int win_rows[kStageWin];
+  int win_off[kStageWin];   // byte offset of window w in a stage
+  int t0_off;               // T_{k-2} rows of the tile (kCheb), -1 otherwise
+  int left_off;             // left rows of the tile (kDotLeft), -1 otherwise
+};
+
+__device__ __forceinline__ uint32_t sm_addr(const void* p)
+{
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count)
+{
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sm_addr(b)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect(uint64_t* b, unsigned bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sm_addr(b)),
+               "r"(bytes)
+               : "memory");
+}
+
+// One try: true once phase `parity` of b has completed; the thread may be suspended for
+// up to about 1 microsecond (the suspend-time hint) while it has not.
+__device__ __forceinline__ bool mbar_test(uint64_t* b, unsigned parity)
+{
+  unsigned ok;
+  asm volatile(
+    "{\n\t.reg .pred p;\n\t"
+    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+    "selp.u32 %0, 1, 0, p;\n\t}"
+    : "=r"(ok)
+    : "r"(sm_addr(b)), "r"(parity), "r"(1000u)
+    : "memory");
+  return ok != 0;
+}
+
+// Wait for phase `parity` of b, for at most 2^20 tries (about a second): false when it
+// did not complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity)
+{
+  for (int it = 0; it < (1 << 20); ++it)
+    if (mbar_test(b, parity))
+      return true;
+  return false;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes,
+                                          uint64_t* b)
+{
+  asm volatile(
+    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+      "r"(sm_addr(dst)),
+    "l"(src), "r"(bytes), "r"(sm_addr(b))
+    : "memory");
+}
+
+__device__ __forceinline__ void fence_async_smem()
+{
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Result index of sum slot k of the threads with lane % (V / 4) == q, H = V / 4 chunks in
+// half a row: vector 2 q + k for k < 2, 2 (q + H) + k - 2 otherwise; P = 2 for the pair
+// sums ([2 v] <T_k|T_k>, [2 v + 1] <T_{k-1}|T_k> in slots 2k', 2k' + 1).
+template <int H, int P>
+struct StageSlots {
+  __device__ __forceinline__ int operator()(int q, int k, int) const
+  {
+    const int kk = k / P;
+    return P * (2 * q + (kk & 1) + (kk >> 1) * 2 * H) + k % P;
+  }
+};
+
+template <int V, int Z, int MODE, int DOT>
+__global__ void __launch_bounds__(kBlock, 2)
+  k_step_staged(Op op, StageLayout sl, const float2* t0, const float2* __restrict__ t1,
+                float2* out, const float2* __restrict__ left, Dot dot)
+{
+  using A = FastArith;
+  constexpr int W = kStageW;
+  constexpr int kTps = V / W;        // threads per site
+  constexpr int TS = kBlock / kTps;  // sites per tile
+  constexpr int RB = V * (int)sizeof(float2);
+  static_assert(kBlock % kTps == 0 && 32 % kTps == 0, "a site's threads share a warp");
+  extern __shared__ __align__(128) unsigned char stage_smem[];
+  const int S = sl.stages;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stage_smem + (size_t)S * sl.stage_bytes);
+  double2* hop = reinterpret_cast<double2*>(bar + kMaxStages);
+  // per code: byte offset in a stage of site 0's neighbour row (-1: gathered from
+  // global memory), and the offset j - i
+  int2* cinfo = reinterpret_cast<int2*>(hop + op.n_codes);
+
+  for (int c = threadIdx.x; c < op.n_codes; c += kBlock) {
+    hop[c] = op.code_hop[c];
+    const int d = op.code_delta[c];
+    int o = -1;
+#pragma unroll
+    for (int w = 0; w < kStageWin; ++w)
+      if (w < sl.nw && o < 0 && d >= sl.win_lo[w] && d <= sl.win_lo[w] + sl.win_rows[w] - TS)
+        o = sl.win_off[w] + (d - sl.win_lo[w]) * RB;
+    cinfo[c] = make_int2(o, d);
+  }
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < S; ++s)
+      mbar_init(bar + s, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    fence_async_smem();
+  }
+  __syncthreads();
+
+  const int n = op.n;
+  const int G = (int)gridDim.x;
+  const int ntiles = (n + TS - 1) / TS;
+  const int mine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
+  // the site's own row (offset 0, in window 0)
+  const int xofs = sl.win_off[0] - sl.win_lo[0] * RB;
+
+  // Thread 0: the copies of this block's tile j into stage j % S.
+  auto produce = [&](int j) {
+    const int s = j % S;
+    unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes;
+    const long long first = (long long)((int)blockIdx.x + j * G) * TS;
+    const long long last = first + TS < n ? first + TS : n;
+    // window w's rows clamped to the vector: [c0, c1)
+    auto clamp = [&](int w, long long& c0, long long& c1) {
+      const long long a = first + sl.win_lo[w], b = a + sl.win_rows[w];
+      c0 = a > 0 ? a : 0;
+      c1 = b < n ? b : n;
+    };
+    unsigned bytes = 0;
+#pragma unroll
+    for (int w = 0; w < kStageWin; ++w) {
+      long long c0, c1;
+      clamp(w, c0, c1);
+      if (w < sl.nw && c1 > c0)
+        bytes += (unsigned)((c1 - c0) * RB);
+    }
+    const unsigned tile_bytes = (unsigned)((last - first) * RB);
+    if constexpr (MODE == kCheb)
+      bytes += tile_bytes;
+    if constexpr (DOT == kDotLeft)
+      bytes += tile_bytes;
+    mbar_arrive_expect(bar + s, bytes);
+#pragma unroll
+    for (int w = 0; w < kStageWin; ++w) {
+      long long c0, c1;
+      clamp(w, c0, c1);
+      if (w < sl.nw && c1 > c0)
+        bulk_load(st + sl.win_off[w] + (c0 - (first + sl.win_lo[w])) * RB,
+                  t1 + (size_t)c0 * V, (unsigned)((c1 - c0) * RB), bar + s);
+    }
+    if constexpr (MODE == kCheb)
+      bulk_load(st + sl.t0_off, t0 + (size_t)first * V, tile_bytes, bar + s);
+    if constexpr (DOT == kDotLeft)
+      bulk_load(st + sl.left_off, left + (size_t)first * V, tile_bytes, bar + s);
+  };
+
+  // This thread computes site l of every tile and the vectors of two 16-byte chunks of
+  // a row, half a row apart: chunk q and q + V/4. On rows of 8 chunks (V = 16) odd
+  // sites take them in the other order, so the 8 threads of a quarter warp (two sites)
+  // read 8 distinct chunks: no shared-memory bank conflict. Slot k < 2 holds vector
+  // 2 ca + k, slot k >= 2 vector 2 cb + k - 2.
+  constexpr int kHalf = V / 4;
+  const int l = (int)threadIdx.x / kTps;
+  const int q = (int)threadIdx.x % kTps;
+  const int sw = (V == 16) ? (l & 1) : 0;
+  const int ca = q + sw * kHalf, cb = q + (1 - sw) * kHalf;
+  auto widen4 = [&](const float4& a, const float4& b, double2 (&y)[W]) {
+    y[0] = make_double2(a.x, a.y);
+    y[1] = make_double2(a.z, a.w);
+    y[2] = make_double2(b.x, b.y);
+    y[3] = make_double2(b.z, b.w);
+  };
+  auto lds4 = [&](const unsigned char* row, double2 (&y)[W]) {
+    widen4(*reinterpret_cast<const float4*>(row + ca * 16),
+           *reinterpret_cast<const float4*>(row + cb * 16), y);
+  };
+  constexpr int kSums = DOT == kDotPair ? 2 * W : W;
+  CSum re[kSums], im[kSums];
+#pragma unroll
+  for (int k = 0; k < kSums; ++k)
+    re[k] = im[k] = CSum{0.0, 0.0};
+
+  // codes and potential of tile j's site l, one tile ahead
+  auto fetch = [&](int j, int (&c)[Z], double& p) {
+    const int i = ((int)blockIdx.x + j * G) * TS + l;
+    if (i < n) {
+#pragma unroll
+      for (int m = 0; m < Z; ++m)
+        c[m] = op.code[(size_t)m * n + i];
+      p = op.pot[i];
+    }
+  };
+  int cc[Z] = {};
+  double p = 0.0;
+  if (mine > 0)
+    fetch(0, cc, p);
+  if (threadIdx.x == 0)
+    for (int j = 0; j < S && j < mine; ++j)
+      produce(j);
+
+  int j = 0;
+  for (; j < mine; ++j) {
+    int cn[Z] = {};
+    double pn = 0.0;
+    if (j + 1 < mine)
+      fetch(j + 1, cn, pn);
+    const int s = j % S;
+    const bool late = !mbar_wait(bar + s, (unsigned)(j / S) & 1u);
+    if (late)
+      atomicOr(op.stage_err, 1u);
+    const unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes + l * RB;
+    const int i = ((int)blockIdx.x + j * G) * TS + l;
+    if (i < n) {
+      double2 x[W];
+      lds4(st + xofs, x);
+      double tr[W], ti[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        tr[k] = A::mul(p, x[k].x);
+        ti[k] = A::mul(p, x[k].y);
+      }
+#pragma unroll
+      for (int m = 0; m < Z; ++m) {
+        const int c = cc[m];
+        const int2 ci = cinfo[c];
+        const double2 h = hop[c];
+        double2 y[W];
+        if (ci.x >= 0) {
+          lds4(st + ci.x, y);
+        } else {
+          const float4* row = reinterpret_cast<const float4*>(t1 + (size_t)(i + ci.y) * V);
+          widen4(__ldg(row + ca), __ldg(row + cb), y);
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          tr[k] = A::add(tr[k], A::cre(h.x, h.y, y[k].x, y[k].y));
+          ti[k] = A::add(ti[k], A::cim(h.x, h.y, y[k].x, y[k].y));
+        }
+      }
+      double2 r[W];
+      if constexpr (MODE == kCheb) {
+        double2 y0[W];
+        lds4(st + sl.t0_off, y0);
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          r[k] = make_double2(A::two_x_minus(A::scale(tr[k], op), y0[k].x),
+                              A::two_x_minus(A::scale(ti[k], op), y0[k].y));
+      } else {
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          r[k] = make_double2(A::scale(tr[k], op), A::scale(ti[k], op));
+      }
+      const float4 oa = make_float4(__double2float_rn(r[0].x), __double2float_rn(r[0].y),
+                                    __double2float_rn(r[1].x), __double2float_rn(r[1].y));
+      const float4 ob = make_float4(__double2float_rn(r[2].x), __double2float_rn(r[2].y),
+                                    __double2float_rn(r[3].x), __double2float_rn(r[3].y));
+      float4* orow = reinterpret_cast<float4*>(out + (size_t)i * V);
+      orow[ca] = oa;
+      orow[cb] = ob;
+      if constexpr (DOT == kDotLeft) {
+        double2 lf[W];
+        lds4(st + sl.left_off, lf);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          re[k].s = fma(r[k].x, lf[k].x, fma(r[k].y, lf[k].y, re[k].s));
+          im[k].s = fma(r[k].y, lf[k].x, fma(-r[k].x, lf[k].y, im[k].s));
+        }
+      } else if constexpr (DOT == kDotPair) {
+        // T_k and T_{k-1} as stored
+        double2 o[W];
+        widen4(oa, ob, o);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          re[2 * k].s = fma(o[k].x, o[k].x, fma(o[k].y, o[k].y, re[2 * k].s));
+          re[2 * k + 1].s = fma(o[k].x, x[k].x, fma(o[k].y, x[k].y, re[2 * k + 1].s));
+          im[2 * k + 1].s = fma(o[k].y, x[k].x, fma(-o[k].x, x[k].y, im[2 * k + 1].s));
+        }
+      }
+    }
+    // stage s is read: thread 0 may refill it; a wait that ran out ends the block's loop
+    if (__syncthreads_or(late))
+      break;
+    if (threadIdx.x == 0 && j + S < mine) {
+      fence_async_smem();
+      produce(j + S);
+    }
+#pragma unroll
+    for (int m = 0; m < Z; ++m)
+      cc[m] = cn[m];
+    p = pn;
+  }
+  if (j < mine && threadIdx.x == 0) {
+    // A wait ran out at tile j: the copies of tiles j .. j + S - 1 may still land in
+    // this block's shared memory; wait for each once more (bounded) before leaving.
+    for (int jj = j; jj < j + S && jj < mine; ++jj)
+      mbar_wait(bar + jj % S, (unsigned)(jj / S) & 1u);
+  }
+  // Slots in the order of even sites (chunk q, then chunk q + V/4) on every thread.
+  if (sw) {
+#pragma unroll
+    for (int k = 0; k < kSums / 2; ++k) {
+      const CSum a = re[k], b = im[k];
+      re[k] = re[k + kSums / 2];
+      im[k] = im[k + kSums / 2];
+      re[k + kSums / 2] = a;
+      im[k + kSums / 2] = b;
+    }
+  }
+  if constexpr (DOT == kDotLeft)
+    dot_finish_w<V, W>(re, im, dot, StageSlots<kHalf, 1>{});
+  else if constexpr (DOT == kDotPair)
+    dot_finish_w<2 * V, 2 * W>(re, im, dot, StageSlots<kHalf, 2>{});
+}
+
+// Stage layout for V vectors: the windows, then T_{k-2} and left as the launch needs them.
+bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayout& sl)
+{
+  const int TS = kBlock * kStageW / V, RB = V * (int)sizeof(float2);
+  sl = StageLayout{};
+  sl.nw = op.stage_nw;
+  int off = 0;
+  for (int w = 0; w < sl.nw; ++w) {
+    sl.win_lo[w] = op.stage_lo[w];
+    sl.win_rows[w] = TS + op.stage_hi[w] - op.stage_lo[w];
+    sl.win_off[w] = off;
+    off += sl.win_rows[w] * RB;
+  }
+  sl.t0_off = sl.left_off = -1;
+  if (mode == kCheb) {
+    sl.t0_off = off;
+    off += TS * RB;
+  }
+  if (dot == kDotLeft) {
+    sl.left_off = off;
+    off += TS * RB;
+  }
+  sl.stage_bytes = (off + 127) / 128 * 128;
+  if (stages <= 1) {
+    // as many stages as fit 104 KB (two blocks per SM), at most kMaxStages
+    stages = (104 << 10) / sl.stage_bytes;
+    stages = stages > kMaxStages ? kMaxStages : stages;
+  }
+  // at most kMaxStages, and no more than fit 200 KB (a block's shared memory is at most
+  // 227 KB, the moment sums and the code table take the rest)
+  const int fit = (200 << 10) / sl.stage_bytes;
+  stages = stages > fit ? fit : stages;
+  sl.stages = stages > kMaxStages ? kMaxStages : stages;
+  return sl.nw > 0 && sl.stages >= 2;
+}
+
+template <int V, int Z, int MODE, int DOT>
+gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
+                         const float2* t1, float2* out, const float2* left, const Dot& d)
+{
+  auto* kernel = k_step_staged<V, Z, MODE, DOT>;
+  const size_t smem = (size_t)sl.stages * sl.stage_bytes + kMaxStages * sizeof(uint64_t) +
+                      (size_t)op.n_codes * (sizeof(double2) + sizeof(int2));
+  static std::mutex mu;
+  static std::unordered_map<size_t, int> per_sm;  // blocks per SM by shared memory size
+  static size_t attr = 0;                         // the kernel's shared memory limit set
+  int bps;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (smem > attr) {
+      GQT_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)smem));
+      attr = smem;
+    }
+    auto it = per_sm.find(smem);
+    if (it == per_sm.end()) {
+      int b = 0;
+      GQT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kBlock, smem));
+      it = per_sm.emplace(smem, b > 0 ? b : 1).first;
+    }
+    bps = it->second;
+  }
+  const int TS = kBlock * kStageW / V;
+  const int ntiles = (op.n + TS - 1) / TS;
+  const int cap = device_info().sms * bps;
+  const int grid = ntiles < cap ? ntiles : cap;
+  kernel<<<grid, kBlock, smem, stream()>>>(op, sl, t0, t1, out, left, d);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+template <int V>
+gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, const void* t0,
+                    const void* t1, void* out, const void* left, const Dot& d)
+{
+  const float2* a0 = (const float2*)t0;
+  const float2* a1 = (const float2*)t1;
+  float2* o = (float2*)out;
+  const float2* lf = (const float2*)left;
+  auto go = [&](auto zc) -> gqt_status {
+    constexpr int Z = decltype(zc)::value;
+    if (dot == kDotPair) {
+      if constexpr (V <= 16) {
+        if (mode == kApply)
+          return launch_staged<V, Z, kApply, kDotPair>(op, sl, a0, a1, o, lf, d);
+        return launch_staged<V, Z, kCheb, kDotPair>(op, sl, a0, a1, o, lf, d);
+      } else {
+        return fail(GQT_ERR_ARG, "symmetric moments: at most 16 vectors per launch");
+      }
+    }
+    if (mode == kApply)
+      return launch_staged<V, Z, kApply, kDotLeft>(op, sl, a0, a1, o, lf, d);
+    return launch_staged<V, Z, kCheb, kDotLeft>(op, sl, a0, a1, o, lf, d);
+  };
+  switch (op.z) {
+    case 3:
+      return go(std::integral_constant<int, 3>{});
+    case 4:
+      return go(std::integral_constant<int, 4>{});
+    default:
+      return go(std::integral_constant<int, 6>{});
+  }
+}
+
+}  // namespace
+
+bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
+                   const void* left)
+{
+  if (op.stage_nw <= 0 || !op.code || !op.stage_err || (mode != kApply && mode != kCheb))
+    return false;
+  // automatic (0): the symmetric loop only. On B200 (graphene 2,097,152 sites, cubic
+  // 256^3; 16 FP32 vectors) its staged pair step was as fast or 41 % faster, while the
+  // staged direct step, at 16 warps per SM against the unstaged step's 32, was 9 % slower.
+  if (op.stage_stages < 0 || (op.stage_stages == 0 && dot != kDotPair))
+    return false;
+  if (nvec != 16 && nvec != 32)
+    return false;
+  if (dot != kDotLeft && dot != kDotPair)
+    return false;
+  if (dot == kDotPair && nvec > 16)
+    return false;
+  if (op.z != 3 && op.z != 4 && op.z != 6)
+    return false;
+  // bulk copies start on 16-byte boundaries (rows are nvec * 8 >= 32 bytes)
+  auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  if (!aligned(t1) || (mode == kCheb && !aligned(t0)) || (dot == kDotLeft && !aligned(left)))
+    return false;
+  StageLayout sl;
+  return stage_layout(op, nvec, mode, dot, op.stage_stages, sl);
+}
+
+gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
+                      const void* t1, void* out, const void* left, const Dot& d)
+{
+  StageLayout sl;
+  if (!stage_layout(op, nvec, mode, dot, op.stage_stages, sl))
+    return fail(GQT_ERR_STATE, "staged step: no stage layout for %d vectors", nvec);
+  switch (nvec) {
+    case 16:
+      return staged_v<16>(op, mode, dot, sl, t0, t1, out, left, d);
+    case 32:
+      return staged_v<32>(op, mode, dot, sl, t0, t1, out, left, d);
+    default:
+      return fail(GQT_ERR_ARG, "staged step: unsupported vector count %d", nvec);
+  }
+}
+
+}  // namespace gqt

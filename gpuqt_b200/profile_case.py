@@ -43,6 +43,8 @@ def main() -> None:
                     help="FP64 moment loop: 0 step by step, S >= 2 wavefront windows of S")
     ap.add_argument("--chunk", type=int, default=0,
                     help="sites per chunk of the wavefront loop (0: the default)")
+    ap.add_argument("--staging", type=int, default=None,
+                    help="staged FP32 step: -1 off, 0 automatic, 1 as many stages as fit, 2..4")
     args = ap.parse_args()
 
     import torch
@@ -77,6 +79,8 @@ def main() -> None:
             H.set_format(g.FORMAT_ELL if args.format == "ell" else g.FORMAT_CODED)
         if args.loop:
             H.set_loop(args.loop, args.chunk)
+        if args.staging is not None:
+            H.set_staging(args.staging)
         tuned = None
         if args.autotune:
             tuned = g.autotune_nvec(H, prec, 20, [V])[1]
@@ -131,6 +135,7 @@ def main() -> None:
                           "n_codes": H.n_codes,
                           "moments": args.moments, "sets": args.sets, "autotune": tuned,
                           "doubled": args.doubled, "loop": list(H.loop),
+                          "staging": H.staging[0], "stage_windows": H.staging[1],
                           "site_moments_per_s": V * sites * args.moments * args.sets / s}))
     finally:
         shutil.rmtree(tmp, ignore_errors=True)

@@ -147,6 +147,22 @@ gqt_status gqt_ham_batch_tile(const gqt_ham* h, int* tile_sites);
  * and halo in chunk positions; halo -2: not applicable). */
 gqt_status gqt_ham_set_loop(gqt_ham* h, int window, int chunk_sites);
 gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo);
+
+/* The staged step of the GQT_FP32 moment loops (no counterpart in the reference) over
+ * the coded operator, for 16 or 32 vectors and rows of 3, 4 or 6 entries. The sites are
+ * cut into tiles; per tile, one thread copies the rows of T_{k-1} its gathers read (a
+ * few windows of frequent neighbour offsets, found at upload), its T_{k-2} rows and
+ * its left rows into shared memory with bulk asynchronous copies, several tiles
+ * ahead, and the block computes from shared memory. Entries whose offset lies in no
+ * window (periodic wraps) gather from global memory. Every T_m is bit-identical to the
+ * unstaged step's; moments agree to FP64 rounding (another summation order).
+ * stages: -1 off; 0 automatic (the default): the symmetric loop (gqt_moments_doubled)
+ * is staged and the direct loop is not, as measured fastest on B200; 1 both loops,
+ * as many stages as fit; 2..4 both loops, that many stages.
+ * gqt_ham_staging reports the setting and the windows (lo/hi: room for 8 ints each,
+ * or null); windows 0 means the step is never staged for this operator. */
+gqt_status gqt_ham_set_staging(gqt_ham* h, int stages);
+gqt_status gqt_ham_staging(const gqt_ham* h, int* stages, int* windows, int* lo, int* hi);
 gqt_status gqt_ham_realisations(const gqt_ham* h, int* count);
 gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
                                double* energy_max);

@@ -89,7 +89,8 @@ def test_autotuner_picks_a_candidate():
 @pytest.mark.parametrize("tile", [256, 512, 1024])
 def test_batch_tile_sizes_give_the_same_moments(tile):
     """Every tile size the step can run with (the autotuner's choice) gives each model
-    the moments of the model run alone, the deferred window reductions included
+    the moments of the model run alone (to 1e-11, the bound of the batch against single
+    runs above: the sums group differently), the deferred window reductions included
     (M = 120 > one window), in the direct and the symmetric (pair) loop."""
     models = _models()
     B = g.Hamiltonian.batch(models)
@@ -106,9 +107,9 @@ def test_batch_tile_sizes_give_the_same_moments(tile):
         for v in (0, 3):
             x = g.Vector.from_host(ph[r][0][v], ph[r][1][v])
             ref = g.moments(H, x, x, M)
-            assert _rel((re[r, v], im[r, v]), ref) <= 1e-12
+            assert _rel((re[r, v], im[r, v]), ref) <= 1e-11
             assert np.max(np.hypot(dr[r, v] - ref[0], di[r, v] - ref[1])) <= (
-                1e-12 * np.max(np.hypot(*ref)))
+                1e-11 * np.max(np.hypot(*ref)))
     with pytest.raises(g.GqtError):
         B.set_batch_tile(384)
     single = g.Hamiltonian(models[0])
