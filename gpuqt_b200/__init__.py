@@ -26,6 +26,7 @@ CLI_PATH = os.path.join(HERE, "lib", "lsqt_b200")
 FP64 = 0
 FP32 = 1
 FP32X = 2  # moment recurrence only: FP32 storage with a BF16 residual
+FP32R = 3  # moment recurrence only: FP32 vectors, hoppings and recurrence; FP64 sums
 FORMAT_ELL = 0    # the reference's ELL arrays
 FORMAT_CODED = 1  # one byte per ELL entry into a table of the distinct entries
 

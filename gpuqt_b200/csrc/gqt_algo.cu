@@ -1017,18 +1017,32 @@ static gqt_status moments_form_run(const gqt_ham* h, const gqt_vec* left, const 
     L.data = same ? R.data : ws_xslot(ws, 1);
     return moments_run(h, &L, &R, M, mu_dev, pair, w);
   }
+  // GQT_FP32R stores its vectors as GQT_FP32 does: FP32 vectors run as they are.
+  const int store = precision == GQT_FP32R ? GQT_FP32 : precision;
+  if (precision == GQT_FP32R) {
+    if (h->n_real > 1)
+      return fail(GQT_ERR_STATE, "%s: the FP32R form runs on one model, not a batch", w);
+    if (right->precision == GQT_FP32X || left->precision == GQT_FP32X ||
+        right->precision == GQT_FP32R || left->precision == GQT_FP32R)
+      return fail(GQT_ERR_ARG, "%s: the FP32R form reads FP32 or FP64 vectors", w);
+    if (right->precision == GQT_FP32 && left->precision == GQT_FP32) {
+      gqt_vec R = *right, L = *left;
+      R.precision = L.precision = GQT_FP32R;
+      return moments_run(h, &L, &R, M, mu_dev, pair, w);
+    }
+  }
   // The converted copies live in workspace slots 4 and 5 of the target form (slots
   // 0-3 are the recurrence and evolution temporaries).
   Workspace& ws = *h->ws;
   const size_t bytes = (size_t)right->n * right->nvec *
-                       (precision == GQT_FP64 ? sizeof(double2) : sizeof(float2));
+                       (store == GQT_FP64 ? sizeof(double2) : sizeof(float2));
   void *lc = nullptr, *rc = nullptr;
-  GQT_TRY(ws_vector(ws, precision, right->nvec, bytes, 5, &rc));
-  GQT_TRY(ws_vector(ws, precision, right->nvec, bytes, 4, &lc));
-  GQT_TRY(convert_data(right->n, right->nvec, right->precision, right->data, precision, rc));
+  GQT_TRY(ws_vector(ws, store, right->nvec, bytes, 5, &rc));
+  GQT_TRY(ws_vector(ws, store, right->nvec, bytes, 4, &lc));
+  GQT_TRY(convert_data(right->n, right->nvec, right->precision, right->data, store, rc));
   const bool same = left->data == right->data;
   if (!same)
-    GQT_TRY(convert_data(left->n, left->nvec, left->precision, left->data, precision, lc));
+    GQT_TRY(convert_data(left->n, left->nvec, left->precision, left->data, store, lc));
   gqt_vec R = *right, L = *left;
   R.precision = L.precision = precision;
   R.bytes = L.bytes = bytes;

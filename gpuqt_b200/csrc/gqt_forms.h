@@ -95,6 +95,8 @@ const FormOps* forms_fp64(int nvec);
 const FormOps* forms_fp32(int nvec);
 // GQT_FP32X: moment loops only (dot, step, step_pair; nvec 1, 4, 16).
 const FormOps* forms_fp32x(int nvec);
+// GQT_FP32R (gqt_stage.cu): moment loops only (dot, step, step_pair; nvec 16 and 32).
+const FormOps* forms_fp32r(int nvec);
 // src (GQT_FP64 or GQT_FP32 storage, `total` elements) into FP32X storage at dst.
 gqt_status convert_to_x(size_t total, int from, const void* src, void* dst, uintptr_t xlo);
 // The coded format's operator kernels (gqt_forms_fp64_coded.cu, gqt_forms_fp32_coded.cu).
@@ -108,17 +110,20 @@ inline const FormOps* form_ops(int precision, int nvec)
     return forms_fp32(nvec);
   if (precision == GQT_FP32X)
     return forms_fp32x(nvec);
+  if (precision == GQT_FP32R)
+    return forms_fp32r(nvec);
   return nullptr;
 }
 
 // The staged step of the FP32 moment loops over the coded operator (gqt_stage.cu): whether
 // it serves this step (op has staging windows, nvec 16 or 32, rows of 3, 4 or 6, dot kDotLeft
-// or kDotPair, 16-byte aligned vectors), and the step itself.
+// or kDotPair, 16-byte aligned vectors), and the step itself; f32 selects the GQT_FP32R
+// arithmetic (the recurrence in FP32) instead of GQT_FP32's.
 bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
-                   const void* left);
+                   const void* left, bool f32 = false);
 gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
-                      const void* t1, void* out, const void* left, const Dot& d);
-
+                      const void* t1, void* out, const void* left, const Dot& d,
+                      bool f32 = false);
 // Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
 // at the number of blocks that are resident at once on all SMs.
 int grid_for(const void* kernel, size_t total);

@@ -189,7 +189,7 @@ extern "C" gqt_status gqt_vec_create(int n, int nvec, int precision, gqt_vec** o
   *out = nullptr;
   if (n <= 0)
     return fail(GQT_ERR_ARG, "gqt_vec_create: number of sites must be > 0 (got %d)", n);
-  if (precision == GQT_FP32X || !form_ops(precision, nvec))
+  if (precision == GQT_FP32X || precision == GQT_FP32R || !form_ops(precision, nvec))
     return fail(GQT_ERR_ARG, "gqt_vec_create: unsupported form (precision %d, %d vectors)",
                 precision, nvec);
   const size_t elem = precision == GQT_FP64 ? sizeof(double2) : sizeof(float2);

@@ -8,14 +8,13 @@
 // reads the rows [t + lo_w, t + TS + hi_w) of it. With the vectors interleaved per site
 // ([site][vector]), each window is one contiguous byte range of T_{k-1}.
 //
-// Thread 0 copies a tile's windows, its T_{k-2} rows and (moment <left|T_k>) its left
-// rows into one of S shared-memory stages with bulk asynchronous copies (cp.async.bulk,
-// completing on the stage's mbarrier), S - 1 tiles ahead of the tile being computed.
-// The compute threads then read every vector operand from shared memory (one 16-byte
-// load per row and thread, conflict-free), so they wait on no global vector load; the
-// codes and the potential of the next tile are loaded one tile ahead into registers.
-// Offsets outside the windows (the periodic wraps: a few rows per lattice line) are
-// gathered from global memory.
+// Thread 0 copies a tile's windows and its T_{k-2} rows into one of S shared-memory
+// stages with bulk asynchronous copies (cp.async.bulk, completing on the stage's
+// mbarrier), S - 1 tiles ahead of the tile being computed. The compute threads read
+// these operands from shared memory (one 16-byte load per row and thread,
+// conflict-free); the codes, the potential and (GQT_FP32R, moment <left|T_k>) the left
+// entries of the next tile are loaded one tile ahead into registers. Offsets outside the windows (the periodic wraps: a
+// few rows per lattice line) are gathered from global memory.
 //
 // Per element the arithmetic is that of k_step_vec with FastArith (src/sigma.cu:33-61's
 // recurrence, the operator in FP64, T_k rounded to FP32 once), so T_k is the unstaged
@@ -25,7 +24,7 @@
 //
 // Every wait on an mbarrier is bounded; one that runs out sets *op.stage_err, stops the
 // block's further copies and is waited for once more (bounded) before the block exits.
-#include "gqt_forms.h"
+#include "gqt_forms_impl.cuh"
 
 #include <mutex>
 #include <unordered_map>
@@ -46,7 +45,6 @@ struct StageLayout {
   int win_rows[kStageWin];
   int win_off[kStageWin];   // byte offset of window w in a stage
   int t0_off;               // T_{k-2} rows of the tile (kCheb), -1 otherwise
-  int left_off;             // left rows of the tile (kDotLeft), -1 otherwise
 };
 
 __device__ __forceinline__ uint32_t sm_addr(const void* p)
@@ -119,7 +117,65 @@ struct StageSlots {
   }
 };
 
-template <int V, int Z, int MODE, int DOT>
+// F32 = false: the GQT_FP32 form (operator and arithmetic in FP64, T_k rounded to FP32).
+// F32 = true: the GQT_FP32R form (recurrence_f32 below).
+// The GQT_FP32R form, a recurrence in FP32. The operator H / E_max (hoppings and
+// potential multiplied by RN(1 / E_max) in FP64) is kept as two FP32 parts, hi =
+// RN_fp32(a) and lo = RN_fp32(a - hi), so that it is not perturbed at FP32 precision (a
+// fixed perturbation of H shifts the spectrum, and its error grows linearly with the
+// moment index); T_k = 2 (H / E_max) T_{k-1} - T_{k-2} is summed with FP32 fused
+// multiply-adds, the hi products and the lo products in two accumulators (neighbours in
+// ELL order) added once per element. The moments are summed in FP64 from the stored
+// FP32 values (the product of two FP32 values is exact in FP64).
+__device__ __forceinline__ float2 split_f32(double a)
+{
+  const float hi = (float)a;
+  return make_float2(hi, (float)(a - (double)hi));
+}
+
+// (hi.x, hi.y, lo.x, lo.y) of a hopping divided by E_max
+__device__ __forceinline__ float4 scaled_hop(double2 h, const Op& op)
+{
+  const float2 x = split_f32(h.x * op.inv_emax), y = split_f32(h.y * op.inv_emax);
+  return make_float4(x.x, y.x, x.y, y.y);
+}
+
+// One vector element of the FP32 recurrence: hi and lo accumulators of both parts.
+struct AccF32 {
+  float r, i, rl, il;
+};
+
+// acc = p x (p = (hi, lo) of the potential divided by E_max)
+__device__ __forceinline__ AccF32 acc_start(float2 p, float2 x)
+{
+  return AccF32{p.x * x.x, p.x * x.y, p.y * x.x, p.y * x.y};
+}
+
+// acc += h y, complex
+__device__ __forceinline__ void cmac_f32(AccF32& a, float4 h, float2 y)
+{
+  a.r = fmaf(h.x, y.x, a.r);
+  a.r = fmaf(-h.y, y.y, a.r);
+  a.i = fmaf(h.x, y.y, a.i);
+  a.i = fmaf(h.y, y.x, a.i);
+  a.rl = fmaf(h.z, y.x, a.rl);
+  a.rl = fmaf(-h.w, y.y, a.rl);
+  a.il = fmaf(h.z, y.y, a.il);
+  a.il = fmaf(h.w, y.x, a.il);
+}
+
+// T_k = 2 acc - T_{k-2} (kCheb), or acc (kApply)
+template <int MODE>
+__device__ __forceinline__ float2 acc_finish(const AccF32& a, float2 y0)
+{
+  const float r = a.r + a.rl, i = a.i + a.il;
+  if constexpr (MODE == kCheb)
+    return make_float2(fmaf(2.0f, r, -y0.x), fmaf(2.0f, i, -y0.y));
+  else
+    return make_float2(r, i);
+}
+
+template <int V, int Z, int MODE, int DOT, bool F32>
 __global__ void __launch_bounds__(kBlock, 2)
   k_step_staged(Op op, StageLayout sl, const float2* t0, const float2* __restrict__ t1,
                 float2* out, const float2* __restrict__ left, Dot dot)
@@ -134,12 +190,15 @@ __global__ void __launch_bounds__(kBlock, 2)
   const int S = sl.stages;
   uint64_t* bar = reinterpret_cast<uint64_t*>(stage_smem + (size_t)S * sl.stage_bytes);
   double2* hop = reinterpret_cast<double2*>(bar + kMaxStages);
+  // GQT_FP32R: the hoppings divided by E_max as FP32 (hi, lo) parts
+  float4* hopf = reinterpret_cast<float4*>(hop + op.n_codes);
   // per code: byte offset in a stage of site 0's neighbour row (-1: gathered from
   // global memory), and the offset j - i
-  int2* cinfo = reinterpret_cast<int2*>(hop + op.n_codes);
+  int2* cinfo = reinterpret_cast<int2*>(hopf + op.n_codes);
 
   for (int c = threadIdx.x; c < op.n_codes; c += kBlock) {
     hop[c] = op.code_hop[c];
+    hopf[c] = scaled_hop(op.code_hop[c], op);
     const int d = op.code_delta[c];
     int o = -1;
 #pragma unroll
@@ -186,8 +245,6 @@ __global__ void __launch_bounds__(kBlock, 2)
     const unsigned tile_bytes = (unsigned)((last - first) * RB);
     if constexpr (MODE == kCheb)
       bytes += tile_bytes;
-    if constexpr (DOT == kDotLeft)
-      bytes += tile_bytes;
     mbar_arrive_expect(bar + s, bytes);
 #pragma unroll
     for (int w = 0; w < kStageWin; ++w) {
@@ -199,8 +256,6 @@ __global__ void __launch_bounds__(kBlock, 2)
     }
     if constexpr (MODE == kCheb)
       bulk_load(st + sl.t0_off, t0 + (size_t)first * V, tile_bytes, bar + s);
-    if constexpr (DOT == kDotLeft)
-      bulk_load(st + sl.left_off, left + (size_t)first * V, tile_bytes, bar + s);
   };
 
   // This thread computes site l of every tile and the vectors of two 16-byte chunks of
@@ -223,26 +278,44 @@ __global__ void __launch_bounds__(kBlock, 2)
     widen4(*reinterpret_cast<const float4*>(row + ca * 16),
            *reinterpret_cast<const float4*>(row + cb * 16), y);
   };
+  auto split4 = [&](const float4& a, const float4& b, float2 (&y)[W]) {
+    y[0] = make_float2(a.x, a.y);
+    y[1] = make_float2(a.z, a.w);
+    y[2] = make_float2(b.x, b.y);
+    y[3] = make_float2(b.z, b.w);
+  };
+  auto ldsf4 = [&](const unsigned char* row, float2 (&y)[W]) {
+    split4(*reinterpret_cast<const float4*>(row + ca * 16),
+           *reinterpret_cast<const float4*>(row + cb * 16), y);
+  };
   constexpr int kSums = DOT == kDotPair ? 2 * W : W;
   CSum re[kSums], im[kSums];
 #pragma unroll
   for (int k = 0; k < kSums; ++k)
     re[k] = im[k] = CSum{0.0, 0.0};
 
-  // codes and potential of tile j's site l, one tile ahead
-  auto fetch = [&](int j, int (&c)[Z], double& p) {
+  // codes, potential and (moment <left|T_k>) this thread's left chunks of tile j's
+  // site l, loaded one tile ahead into registers: left is read only by the moment, so
+  // it takes no shared memory
+  auto fetch = [&](int j, int (&c)[Z], double& p, float4& la, float4& lb) {
     const int i = ((int)blockIdx.x + j * G) * TS + l;
     if (i < n) {
 #pragma unroll
       for (int m = 0; m < Z; ++m)
         c[m] = op.code[(size_t)m * n + i];
       p = op.pot[i];
+      if constexpr (DOT == kDotLeft && F32) {
+        const float4* row = reinterpret_cast<const float4*>(left + (size_t)i * V);
+        la = __ldg(row + ca);
+        lb = __ldg(row + cb);
+      }
     }
   };
   int cc[Z] = {};
   double p = 0.0;
+  float4 la = {}, lb = {};
   if (mine > 0)
-    fetch(0, cc, p);
+    fetch(0, cc, p, la, lb);
   if (threadIdx.x == 0)
     for (int j = 0; j < S && j < mine; ++j)
       produce(j);
@@ -251,15 +324,69 @@ __global__ void __launch_bounds__(kBlock, 2)
   for (; j < mine; ++j) {
     int cn[Z] = {};
     double pn = 0.0;
+    float4 lan = {}, lbn = {};
     if (j + 1 < mine)
-      fetch(j + 1, cn, pn);
+      fetch(j + 1, cn, pn, lan, lbn);
     const int s = j % S;
     const bool late = !mbar_wait(bar + s, (unsigned)(j / S) & 1u);
     if (late)
       atomicOr(op.stage_err, 1u);
     const unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes + l * RB;
     const int i = ((int)blockIdx.x + j * G) * TS + l;
-    if (i < n) {
+    if (F32 && i < n) {
+      float2 x[W];
+      ldsf4(st + xofs, x);
+      const float2 pf = split_f32(p * op.inv_emax);
+      AccF32 acc[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        acc[k] = acc_start(pf, x[k]);
+#pragma unroll
+      for (int m = 0; m < Z; ++m) {
+        const int c = cc[m];
+        const int2 ci = cinfo[c];
+        const float4 h = hopf[c];
+        float2 y[W];
+        if (ci.x >= 0) {
+          ldsf4(st + ci.x, y);
+        } else {
+          const float4* row = reinterpret_cast<const float4*>(t1 + (size_t)(i + ci.y) * V);
+          split4(__ldg(row + ca), __ldg(row + cb), y);
+        }
+#pragma unroll
+        for (int k = 0; k < W; ++k)
+          cmac_f32(acc[k], h, y[k]);
+      }
+      float2 y0[W] = {};
+      if constexpr (MODE == kCheb)
+        ldsf4(st + sl.t0_off, y0);
+      float2 r[W];
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        r[k] = acc_finish<MODE>(acc[k], y0[k]);
+      float4* orow = reinterpret_cast<float4*>(out + (size_t)i * V);
+      orow[ca] = make_float4(r[0].x, r[0].y, r[1].x, r[1].y);
+      orow[cb] = make_float4(r[2].x, r[2].y, r[3].x, r[3].y);
+      if constexpr (DOT == kDotLeft) {
+        float2 lf[W];
+        split4(la, lb, lf);
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const double rx = r[k].x, ry = r[k].y, lx = lf[k].x, ly = lf[k].y;
+          re[k].s = fma(rx, lx, fma(ry, ly, re[k].s));
+          im[k].s = fma(ry, lx, fma(-rx, ly, im[k].s));
+        }
+      } else if constexpr (DOT == kDotPair) {
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+          const double ox = r[k].x, oy = r[k].y, xx = x[k].x, xy = x[k].y;
+          re[2 * k].s = fma(ox, ox, fma(oy, oy, re[2 * k].s));
+          re[2 * k + 1].s = fma(ox, xx, fma(oy, xy, re[2 * k + 1].s));
+          im[2 * k + 1].s = fma(oy, xx, fma(-ox, xy, im[2 * k + 1].s));
+        }
+      }
+    }
+    if (!F32 && i < n) {
       double2 x[W];
       lds4(st + xofs, x);
       double tr[W], ti[W];
@@ -307,8 +434,10 @@ __global__ void __launch_bounds__(kBlock, 2)
       orow[ca] = oa;
       orow[cb] = ob;
       if constexpr (DOT == kDotLeft) {
+        // (the FP64-arithmetic variant loads left here: held a tile ahead it spilled)
+        const float4* lrow = reinterpret_cast<const float4*>(left + (size_t)i * V);
         double2 lf[W];
-        lds4(st + sl.left_off, lf);
+        widen4(__ldg(lrow + ca), __ldg(lrow + cb), lf);
 #pragma unroll
         for (int k = 0; k < W; ++k) {
           re[k].s = fma(r[k].x, lf[k].x, fma(r[k].y, lf[k].y, re[k].s));
@@ -337,6 +466,8 @@ __global__ void __launch_bounds__(kBlock, 2)
     for (int m = 0; m < Z; ++m)
       cc[m] = cn[m];
     p = pn;
+    la = lan;
+    lb = lbn;
   }
   if (j < mine && threadIdx.x == 0) {
     // A wait ran out at tile j: the copies of tiles j .. j + S - 1 may still land in
@@ -374,13 +505,9 @@ bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayou
     sl.win_off[w] = off;
     off += sl.win_rows[w] * RB;
   }
-  sl.t0_off = sl.left_off = -1;
+  sl.t0_off = -1;
   if (mode == kCheb) {
     sl.t0_off = off;
-    off += TS * RB;
-  }
-  if (dot == kDotLeft) {
-    sl.left_off = off;
     off += TS * RB;
   }
   sl.stage_bytes = (off + 127) / 128 * 128;
@@ -397,13 +524,13 @@ bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayou
   return sl.nw > 0 && sl.stages >= 2;
 }
 
-template <int V, int Z, int MODE, int DOT>
+template <int V, int Z, int MODE, int DOT, bool F32>
 gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
                          const float2* t1, float2* out, const float2* left, const Dot& d)
 {
-  auto* kernel = k_step_staged<V, Z, MODE, DOT>;
+  auto* kernel = k_step_staged<V, Z, MODE, DOT, F32>;
   const size_t smem = (size_t)sl.stages * sl.stage_bytes + kMaxStages * sizeof(uint64_t) +
-                      (size_t)op.n_codes * (sizeof(double2) + sizeof(int2));
+                      (size_t)op.n_codes * (sizeof(double2) + sizeof(int2) + sizeof(float4));
   static std::mutex mu;
   static std::unordered_map<size_t, int> per_sm;  // blocks per SM by shared memory size
   static size_t attr = 0;                         // the kernel's shared memory limit set
@@ -433,7 +560,7 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
   return GQT_OK;
 }
 
-template <int V>
+template <int V, bool F32>
 gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, const void* t0,
                     const void* t1, void* out, const void* left, const Dot& d)
 {
@@ -446,15 +573,15 @@ gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, cons
     if (dot == kDotPair) {
       if constexpr (V <= 16) {
         if (mode == kApply)
-          return launch_staged<V, Z, kApply, kDotPair>(op, sl, a0, a1, o, lf, d);
-        return launch_staged<V, Z, kCheb, kDotPair>(op, sl, a0, a1, o, lf, d);
+          return launch_staged<V, Z, kApply, kDotPair, F32>(op, sl, a0, a1, o, lf, d);
+        return launch_staged<V, Z, kCheb, kDotPair, F32>(op, sl, a0, a1, o, lf, d);
       } else {
         return fail(GQT_ERR_ARG, "symmetric moments: at most 16 vectors per launch");
       }
     }
     if (mode == kApply)
-      return launch_staged<V, Z, kApply, kDotLeft>(op, sl, a0, a1, o, lf, d);
-    return launch_staged<V, Z, kCheb, kDotLeft>(op, sl, a0, a1, o, lf, d);
+      return launch_staged<V, Z, kApply, kDotLeft, F32>(op, sl, a0, a1, o, lf, d);
+    return launch_staged<V, Z, kCheb, kDotLeft, F32>(op, sl, a0, a1, o, lf, d);
   };
   switch (op.z) {
     case 3:
@@ -469,14 +596,14 @@ gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, cons
 }  // namespace
 
 bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
-                   const void* left)
+                   const void* left, bool f32)
 {
   if (op.stage_nw <= 0 || !op.code || !op.stage_err || (mode != kApply && mode != kCheb))
     return false;
   // automatic (0): the symmetric loop only. On B200 (graphene 2,097,152 sites, cubic
   // 256^3; 16 FP32 vectors) its staged pair step was as fast or 41 % faster, while the
   // staged direct step, at 16 warps per SM against the unstaged step's 32, was 9 % slower.
-  if (op.stage_stages < 0 || (op.stage_stages == 0 && dot != kDotPair))
+  if (op.stage_stages < 0 || (op.stage_stages == 0 && dot != kDotPair && !f32))
     return false;
   if (nvec != 16 && nvec != 32)
     return false;
@@ -495,18 +622,190 @@ bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, co
 }
 
 gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
-                      const void* t1, void* out, const void* left, const Dot& d)
+                      const void* t1, void* out, const void* left, const Dot& d, bool f32)
 {
   StageLayout sl;
   if (!stage_layout(op, nvec, mode, dot, op.stage_stages, sl))
     return fail(GQT_ERR_STATE, "staged step: no stage layout for %d vectors", nvec);
   switch (nvec) {
     case 16:
-      return staged_v<16>(op, mode, dot, sl, t0, t1, out, left, d);
+      return f32 ? staged_v<16, true>(op, mode, dot, sl, t0, t1, out, left, d)
+                 : staged_v<16, false>(op, mode, dot, sl, t0, t1, out, left, d);
     case 32:
-      return staged_v<32>(op, mode, dot, sl, t0, t1, out, left, d);
+      return f32 ? staged_v<32, true>(op, mode, dot, sl, t0, t1, out, left, d)
+                 : staged_v<32, false>(op, mode, dot, sl, t0, t1, out, left, d);
     default:
       return fail(GQT_ERR_ARG, "staged step: unsupported vector count %d", nvec);
+  }
+}
+
+
+// ------------------------------------------------------------------ the GQT_FP32R form
+namespace {
+
+// The GQT_FP32R step without staging (the ELL arrays, operators without windows, vectors
+// not on 16-byte boundaries): grid-stride items of one site and 4 consecutive vectors,
+// with the staged step's arithmetic (entries past a row's length are skipped).
+// three blocks per SM (85 registers) on rows of known length; two on rows of unknown
+// length, which spilled at three
+template <int Z>
+constexpr int r_min_blocks()
+{
+  return Z > 0 ? 3 : 2;
+}
+
+template <int V, int Z, int MODE, int DOT, bool C>
+__global__ void __launch_bounds__(kBlock, r_min_blocks<Z>()) k_step_r(Op op, const float2* t0,
+                                                   const float2* __restrict__ t1, float2* out,
+                                                   const float2* __restrict__ left, Dot dot)
+{
+  constexpr int W = 4;
+  constexpr int kTps = V / W;
+  const Tables tb = load_tables<C>(op);
+  auto ld4 = [](const float2* p, float2 (&y)[W]) {
+    const float4 a = *reinterpret_cast<const float4*>(p);
+    const float4 b = *reinterpret_cast<const float4*>(p + 2);
+    y[0] = make_float2(a.x, a.y);
+    y[1] = make_float2(a.z, a.w);
+    y[2] = make_float2(b.x, b.y);
+    y[3] = make_float2(b.z, b.w);
+  };
+  constexpr int kSums = DOT == kDotPair ? 2 * W : W;
+  CSum re[kSums], im[kSums];
+#pragma unroll
+  for (int k = 0; k < kSums; ++k)
+    re[k] = im[k] = CSum{0.0, 0.0};
+  const size_t items = (size_t)op.n * kTps;
+  for (size_t g = (size_t)blockIdx.x * kBlock + threadIdx.x; g < items;
+       g += (size_t)gridDim.x * kBlock) {
+    const int i = (int)(g / kTps);
+    const size_t base = (size_t)i * V + (size_t)(g % kTps) * W;
+    float2 x[W];
+    ld4(t1 + base, x);
+    const float2 pf = split_f32(op.pot[i] * op.inv_emax);
+    AccF32 acc[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      acc[k] = acc_start(pf, x[k]);
+    const int cnt = op.uniform ? (Z > 0 ? Z : op.z) : op.nn[i];
+    for_entries<Z>(cnt, [&](int m) {
+      int j, c;
+      double2 h;
+      ell_entry<C>(op, tb, (size_t)m * op.n + i, i, j, h, c);
+      const float4 hf = scaled_hop(h, op);
+      float2 y[W];
+      ld4(t1 + (size_t)j * V + (base - (size_t)i * V), y);
+#pragma unroll
+      for (int k = 0; k < W; ++k)
+        cmac_f32(acc[k], hf, y[k]);
+    });
+    float2 y0[W] = {};
+    if constexpr (MODE == kCheb)
+      ld4(t0 + base, y0);
+    float2 r[W];
+#pragma unroll
+    for (int k = 0; k < W; ++k)
+      r[k] = acc_finish<MODE>(acc[k], y0[k]);
+    reinterpret_cast<float4*>(out + base)[0] = make_float4(r[0].x, r[0].y, r[1].x, r[1].y);
+    reinterpret_cast<float4*>(out + base)[1] = make_float4(r[2].x, r[2].y, r[3].x, r[3].y);
+    if constexpr (DOT == kDotLeft) {
+      float2 lf[W];
+      ld4(left + base, lf);
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const double rx = r[k].x, ry = r[k].y, lx = lf[k].x, ly = lf[k].y;
+        re[k].s = fma(rx, lx, fma(ry, ly, re[k].s));
+        im[k].s = fma(ry, lx, fma(-rx, ly, im[k].s));
+      }
+    } else {
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        const double ox = r[k].x, oy = r[k].y, xx = x[k].x, xy = x[k].y;
+        re[2 * k].s = fma(ox, ox, fma(oy, oy, re[2 * k].s));
+        re[2 * k + 1].s = fma(ox, xx, fma(oy, xy, re[2 * k + 1].s));
+        im[2 * k + 1].s = fma(oy, xx, fma(-ox, xy, im[2 * k + 1].s));
+      }
+    }
+  }
+  if constexpr (DOT == kDotLeft)
+    dot_finish_w<V, W>(re, im, dot);
+  else
+    dot_finish_w<2 * V, 2 * W>(re, im, dot);
+}
+
+template <int V, int DOT, bool C>
+gqt_status run_r(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                 const void* left, const Dot& d)
+{
+  if (C && stage_applies(op, V, mode, DOT, t0, t1, left, true))
+    return stage_step(op, V, mode, DOT, t0, t1, out, left, d, true);
+  const float2* a0 = (const float2*)t0;
+  const float2* a1 = (const float2*)t1;
+  float2* o = (float2*)out;
+  const float2* lf = (const float2*)left;
+  const size_t items = (size_t)op.n * (V / 4);
+  return with_z(op.z, [&](auto zc) -> gqt_status {
+    constexpr int Z = decltype(zc)::value;
+    if (mode == kApply)
+      return launch_op(k_step_r<V, Z, kApply, DOT, C>, items, op, a0, a1, o, lf, d);
+    return launch_op(k_step_r<V, Z, kCheb, DOT, C>, items, op, a0, a1, o, lf, d);
+  });
+}
+
+template <int V, bool C>
+gqt_status step_r(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                  const void* left, const Dot* dot)
+{
+  if (!dot)
+    return fail(GQT_ERR_ARG, "the FP32R form runs moment loops only");
+  return run_r<V, kDotLeft, C>(op, mode, t0, t1, out, left, *dot);
+}
+
+template <int V, bool C>
+gqt_status step_pair_r(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                       const Dot& d)
+{
+  if constexpr (V > 16)
+    return fail(GQT_ERR_ARG, "symmetric moments: at most 16 vectors per launch (got %d)", V);
+  else
+    return run_r<V, kDotPair, C>(op, mode, t0, t1, out, nullptr, d);
+}
+
+template <int V>
+gqt_status dot_r(size_t total, const void* state, const void* left, const Dot& d)
+{
+  return launch(k_dot<float2, V>, total, total, (const float2*)state, (const float2*)left, d);
+}
+
+template <int V>
+const FormOps* table_r()
+{
+  static const FormOps t = [] {
+    FormOps f{};
+    f.precision = GQT_FP32R;
+    f.nvec = V;
+    f.elem_bytes = sizeof(float2);
+    f.fmt[0].step = step_r<V, false>;
+    f.fmt[0].step_pair = step_pair_r<V, false>;
+    f.fmt[1].step = step_r<V, true>;
+    f.fmt[1].step_pair = step_pair_r<V, true>;
+    f.dot = dot_r<V>;
+    return f;
+  }();
+  return &t;
+}
+
+}  // namespace
+
+const FormOps* forms_fp32r(int nvec)
+{
+  switch (nvec) {
+    case 16:
+      return table_r<16>();
+    case 32:
+      return table_r<32>();
+    default:
+      return nullptr;
   }
 }
 

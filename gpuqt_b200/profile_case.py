@@ -51,10 +51,11 @@ def main() -> None:
 
     import gpuqt_b200 as g
 
-    mo = re.fullmatch(r"(fp64|fp32)(?:v(\d+))?", args.form)
+    mo = re.fullmatch(r"(fp64|fp32r|fp32)(?:v(\d+))?", args.form)
     if not mo:
         raise SystemExit(f"unknown form {args.form}")
-    prec = g.FP64 if mo.group(1) == "fp64" else g.FP32
+    prec = g.FP64 if mo.group(1) == "fp64" else g.FP32  # storage of the vectors
+    run_prec = g.FP32R if mo.group(1) == "fp32r" else None  # form of the recurrence
     V = int(mo.group(2) or 1)
     tmp = tempfile.mkdtemp(prefix="gqt_prof_")
     try:
@@ -117,10 +118,10 @@ def main() -> None:
             return
         if args.doubled:
             def one():
-                g.moments_doubled_device(H, X, args.moments, mu.data_ptr())
+                g.moments_doubled_device(H, X, args.moments, mu.data_ptr(), precision=run_prec)
         else:
             def one():
-                g.moments_device(H, X, X, args.moments, mu.data_ptr())
+                g.moments_device(H, X, X, args.moments, mu.data_ptr(), precision=run_prec)
         one()
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -50,7 +50,13 @@ enum {
    * FP64's 16, about 32 significant bits), with the FP64 operator and FP64 sums.
    * DOS and VAC agree with FP64 to about 1e-8 pointwise, where FP32 storage reaches a
    * few 1e-6 at late VAC times. Vectors of this form cannot be created. */
-  GQT_FP32X = 2
+  GQT_FP32X = 2,
+  /* No counterpart in the reference. A form of the moment recurrence only (as
+   * GQT_FP32X; 16 or 32 vectors per launch): FP32 vectors and FP32 hoppings (divided
+   * by energy_max in FP64, then rounded once), the Chebyshev recurrence in FP32, and
+   * the moments summed in FP64 from the stored FP32 values. Runs on GQT_FP32 vectors
+   * as they are, or on FP32 copies of GQT_FP64 ones. */
+  GQT_FP32R = 3
 };
 
 typedef struct gqt_ham gqt_ham;
