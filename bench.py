@@ -641,7 +641,43 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
          "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (r32[0], i32[0])),
          "speedup_vs_fp64": rate32_dbl / rate64},
         **pair_roofline(rate32_dbl, fp32_pair_bytes_per_site_vector_step(16, coded=coded)))
-    del X16
+    # GQT_FP32R (the recurrence in FP32, FP64 sums) on the same FP32 vectors: same bytes
+    # as the FP32-storage form, direct and symmetric loops.
+    mu = torch.empty(2 * M * 16, dtype=torch.float64, device="cuda")
+    for _ in range(2):
+        g.moments_device(H, X16, X16, M, mu.data_ptr(), precision=g.FP32R)
+    a, b = ev()
+    a.record(stream)
+    for _ in range(3):
+        g.moments_device(H, X16, X16, M, mu.data_ptr(), precision=g.FP32R)
+    b.record(stream)
+    torch.cuda.synchronize()
+    rate_r = 16 * n * M * 3 / (a.elapsed_time(b) / 1e3)
+    mh = mu.view(M, 16, 2).cpu().numpy()
+    br = fp32_bytes_per_site_vector(16, coded=coded)
+    ach = br * rate_r / 1e9
+    out["fp32r_v16"] = {"site_moments_per_s": rate_r, "vectors_per_launch": 16,
+                        "achieved_gbs": ach, "frac": ach / hbm_peak,
+                        "bytes_per_site_moment": br,
+                        "dos_err_vs_fp64": dos_error(g, m, (r64, i64),
+                                                     (mh[:, 0, 0].copy(), mh[:, 0, 1].copy())),
+                        "speedup_vs_fp64": rate_r / rate64}
+    g.moments_doubled_device(H, X16, M, mu.data_ptr(), precision=g.FP32R)
+    a, b = ev()
+    a.record(stream)
+    for _ in range(3):
+        g.moments_doubled_device(H, X16, M, mu.data_ptr(), precision=g.FP32R)
+    b.record(stream)
+    torch.cuda.synchronize()
+    rate_rd = 16 * n * M * 3 / (a.elapsed_time(b) / 1e3)
+    mh = mu.view(M, 16, 2).cpu().numpy()
+    out["fp32r_v16_doubled"] = dict(
+        {"site_moments_per_s": rate_rd, "vectors_per_launch": 16,
+         "dos_err_vs_fp64": dos_error(g, m, (r64, i64), (mh[:, 0, 0].copy(),
+                                                         mh[:, 0, 1].copy())),
+         "speedup_vs_fp64": rate_rd / rate64},
+        **pair_roofline(rate_rd, fp32_pair_bytes_per_site_vector_step(16, coded=coded)))
+    del X16, mu
     ach = fp64_bytes_per_site(coded=False) * rate64_ell / 1e9
     out["fp64_v1_ell"] = {"site_moments_per_s": rate64_ell, "achieved_gbs": ach,
                           "frac": ach / hbm_peak,
@@ -672,7 +708,17 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
         "dos_err_fp32_v16": d32["dos_err_vs_fp64"],
         "speedup_fp32x_v16_direct": out["fp32x_v16"]["speedup_vs_fp64"],
         "frac_fp32x_v16_direct": out["fp32x_v16"]["frac"],
-        "met_like_for_like": bool(max(ratio_direct, ratio_dbl) >= 3.0 and
+        "speedup_fp32r_direct": out["fp32r_v16"]["site_moments_per_s"] / rate64,
+        "speedup_fp32r_doubled": out["fp32r_v16_doubled"]["site_moments_per_s"] / rate64_dbl,
+        "speedup_fp32r_doubled_over_fp64_direct":
+            out["fp32r_v16_doubled"]["site_moments_per_s"] / rate64,
+        "frac_fp32r_v16_direct": out["fp32r_v16"]["frac"],
+        "frac_fp32r_v16_doubled": out["fp32r_v16_doubled"]["frac"],
+        "dos_err_fp32r_v16": out["fp32r_v16"]["dos_err_vs_fp64"],
+        "met_like_for_like": bool(max(ratio_direct, ratio_dbl,
+                                      out["fp32r_v16"]["site_moments_per_s"] / rate64,
+                                      out["fp32r_v16_doubled"]["site_moments_per_s"] /
+                                      rate64_dbl) >= 3.0 and
                                   d32["frac"] >= 0.7 and out["fp64_v1"]["frac"] >= 0.7),
         "note": "while both forms are HBM-bound the like-for-like ratio is capped by "
                 "the byte models (byte_ceiling_*): FP32 storage keeps four 8-byte vector "
@@ -801,6 +847,26 @@ def measure_cubic(g, torch, tmp, stream, hbm_peak, vectors=16):
                            "k_cheb2x_frac": gb_x / hbm_peak, "k_cheb2x_gbs": gb_x},
         "dos_err_fp32_vs_fp64": dos,
     }
+    # GQT_FP32R on the initial FP32 vectors again (the evolution parts above changed X):
+    # the DOS moment set, direct and symmetric
+    X.upload(np.stack([v[0] for v in vecs]), np.stack([v[1] for v in vecs]))
+    msr = timed(lambda: g.moments_device(H, X, X, M, mu32.data_ptr(), precision=g.FP32R))
+    mu_h = mu32.view(M, vectors, 2).cpu().numpy()
+    rate_r = vectors * n * M / (msr / 1e3)
+    msd_r = timed(lambda: g.moments_doubled_device(H, X, M, mu32.data_ptr(),
+                                                   precision=g.FP32R))
+    rate_rd = vectors * n * M / (msd_r / 1e3)
+    ach = rate_r * b32 / 1e9
+    bp = fp32_pair_bytes_per_site_vector_step(vectors, z=z, coded=coded)
+    out["fp32r_v16"] = {"vectors_per_launch": vectors, "dos_site_moments_per_s": rate_r,
+                        "ms_dos_set": msr, "bytes_per_site_moment": b32,
+                        "achieved_gbs": ach, "frac": ach / hbm_peak,
+                        "dos_err_vs_fp64": P.compare(g, m, (r64, i64),
+                                                     (mu_h[:, 0, 0].copy(),
+                                                      mu_h[:, 0, 1].copy())),
+                        "doubled_site_moments_per_s": rate_rd,
+                        "doubled_frac": rate_rd / 2 * bp / 1e9 / hbm_peak,
+                        "speedup_dos": rate_r / rate64}
     del X, mu32
     # VAC moment sets of the first two correlation steps, FP32 storage against FP64
     # (vector 0; states evolved in FP64, as the library's FP32 form does).

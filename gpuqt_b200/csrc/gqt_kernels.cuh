@@ -339,7 +339,8 @@ __device__ __forceinline__ void grid_combine(const double* partials, int nblocks
   const int v = threadIdx.x % V;
   constexpr int kStride = kBlock / V;
   CSum r{0.0, 0.0}, i{0.0, 0.0};
-  int b = threadIdx.x / V;
+  // threads past kBlock (a block with a producer warp) take no part
+  int b = threadIdx.x < kBlock ? (int)threadIdx.x / V : nblocks;
   // Four blocks' partials are loaded before they are merged (in block order), so the
   // L2 round trips overlap.
   for (; b + 3 * kStride < nblocks; b += 4 * kStride) {
@@ -368,7 +369,7 @@ __device__ __forceinline__ void grid_combine(const double* partials, int nblocks
     csum_merge(i, shfl_xor(i, off));
   }
   __syncthreads();
-  if (lane < V) {
+  if (lane < V && warp < kWarps) {
     sh[warp][lane][0] = r.s;
     sh[warp][lane][1] = r.c;
     sh[warp][lane][2] = i.s;
@@ -396,14 +397,15 @@ struct ContigSlots {
 // v < V. Slot k of a thread holds the sums of vector map(q, k, W), q = lane % (V/W)
 // (by default W consecutive vectors from q W). Must be reached by every thread of the
 // block.
-template <int V, int W, class Map = ContigSlots>
+// Only the first NW warps hold sums (a block may have more warps, which take no part).
+template <int V, int W, class Map = ContigSlots, int NW = kBlock / 32>
 __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const Dot& dot,
                                              Map map = Map{})
 {
   static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "V must be a power of two <= 32");
   static_assert(W >= 1 && W <= V && V % W == 0, "W must divide V");
   constexpr int kTps = V / W;  // threads sharing one site
-  constexpr int kWarps = kBlock / 32;
+  constexpr int kWarps = NW;
   __shared__ double sh[kWarps][V][4];
   __shared__ unsigned is_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -416,7 +418,7 @@ __device__ __forceinline__ void dot_finish_w(CSum (&re)[W], CSum (&im)[W], const
       csum_merge(im[k], shfl_xor(im[k], off));
     }
   }
-  if (lane < kTps) {
+  if (lane < kTps && warp < kWarps) {
 #pragma unroll
     for (int k = 0; k < W; ++k) {
       const int v = map(lane, k, W);

@@ -8,9 +8,10 @@
 // reads the rows [t + lo_w, t + TS + hi_w) of it. With the vectors interleaved per site
 // ([site][vector]), each window is one contiguous byte range of T_{k-1}.
 //
-// Thread 0 copies a tile's windows and its T_{k-2} rows into one of S shared-memory
-// stages with bulk asynchronous copies (cp.async.bulk, completing on the stage's
-// mbarrier), S - 1 tiles ahead of the tile being computed. The compute threads read
+// One producer thread (a warp of its own) copies a tile's windows and its T_{k-2} rows
+// into one of S shared-memory stages with bulk asynchronous copies (cp.async.bulk,
+// completing on the stage's full mbarrier), up to S tiles ahead of the compute warps,
+// which release a stage through its empty mbarrier. The compute threads read
 // these operands from shared memory (one 16-byte load per row and thread,
 // conflict-free); the codes, the potential and (GQT_FP32R, moment <left|T_k>) the left
 // entries of the next tile are loaded one tile ahead into registers. Offsets outside the windows (the periodic wraps: a
@@ -22,8 +23,9 @@
 // table (offset 0, hopping 0) and add an exact zero instead of being skipped. The
 // moments are the same per-thread FP64 sums taken over the sites in another order.
 //
-// Every wait on an mbarrier is bounded; one that runs out sets *op.stage_err, stops the
-// block's further copies and is waited for once more (bounded) before the block exits.
+// Every wait on an mbarrier is bounded; one that runs out sets *op.stage_err and ends
+// the loop of the warp (or of the producer, which stops copying) that waited; the
+// producer waits once more (bounded) for every copy it issued before the block exits.
 #include "gqt_forms_impl.cuh"
 
 #include <mutex>
@@ -34,6 +36,8 @@ namespace gqt {
 namespace {
 
 constexpr int kMaxStages = 4;
+constexpr int kComputeWarps = kBlock / 32;
+constexpr int kStageThreads = kBlock + 32;  // the compute warps and one producer warp
 constexpr int kStageW = 4;  // vectors per thread: two 16-byte chunks of a row
 
 // Byte layout of one stage for a launch (host-computed from the operator's windows).
@@ -67,6 +71,11 @@ __device__ __forceinline__ void mbar_arrive_expect(uint64_t* b, unsigned bytes)
 
 // One try: true once phase `parity` of b has completed; the thread may be suspended for
 // up to about 1 microsecond (the suspend-time hint) while it has not.
+__device__ __forceinline__ void mbar_arrive(uint64_t* b)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(sm_addr(b)) : "memory");
+}
+
 __device__ __forceinline__ bool mbar_test(uint64_t* b, unsigned parity)
 {
   unsigned ok;
@@ -176,7 +185,7 @@ __device__ __forceinline__ float2 acc_finish(const AccF32& a, float2 y0)
 }
 
 template <int V, int Z, int MODE, int DOT, bool F32>
-__global__ void __launch_bounds__(kBlock, 2)
+__global__ void __launch_bounds__(kStageThreads, 2)
   k_step_staged(Op op, StageLayout sl, const float2* t0, const float2* __restrict__ t1,
                 float2* out, const float2* __restrict__ left, Dot dot)
 {
@@ -188,15 +197,17 @@ __global__ void __launch_bounds__(kBlock, 2)
   static_assert(kBlock % kTps == 0 && 32 % kTps == 0, "a site's threads share a warp");
   extern __shared__ __align__(128) unsigned char stage_smem[];
   const int S = sl.stages;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(stage_smem + (size_t)S * sl.stage_bytes);
-  double2* hop = reinterpret_cast<double2*>(bar + kMaxStages);
+  // per stage: full (the copies have landed) and empty (every compute warp has read it)
+  uint64_t* full = reinterpret_cast<uint64_t*>(stage_smem + (size_t)S * sl.stage_bytes);
+  uint64_t* empty = full + kMaxStages;
+  double2* hop = reinterpret_cast<double2*>(empty + kMaxStages);
   // GQT_FP32R: the hoppings divided by E_max as FP32 (hi, lo) parts
   float4* hopf = reinterpret_cast<float4*>(hop + op.n_codes);
   // per code: byte offset in a stage of site 0's neighbour row (-1: gathered from
   // global memory), and the offset j - i
   int2* cinfo = reinterpret_cast<int2*>(hopf + op.n_codes);
 
-  for (int c = threadIdx.x; c < op.n_codes; c += kBlock) {
+  for (int c = threadIdx.x; c < op.n_codes; c += blockDim.x) {
     hop[c] = op.code_hop[c];
     hopf[c] = scaled_hop(op.code_hop[c], op);
     const int d = op.code_delta[c];
@@ -208,8 +219,10 @@ __global__ void __launch_bounds__(kBlock, 2)
     cinfo[c] = make_int2(o, d);
   }
   if (threadIdx.x == 0) {
-    for (int s = 0; s < S; ++s)
-      mbar_init(bar + s, 1);
+    for (int s = 0; s < S; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, kComputeWarps);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     fence_async_smem();
   }
@@ -245,17 +258,17 @@ __global__ void __launch_bounds__(kBlock, 2)
     const unsigned tile_bytes = (unsigned)((last - first) * RB);
     if constexpr (MODE == kCheb)
       bytes += tile_bytes;
-    mbar_arrive_expect(bar + s, bytes);
+    mbar_arrive_expect(full + s, bytes);
 #pragma unroll
     for (int w = 0; w < kStageWin; ++w) {
       long long c0, c1;
       clamp(w, c0, c1);
       if (w < sl.nw && c1 > c0)
         bulk_load(st + sl.win_off[w] + (c0 - (first + sl.win_lo[w])) * RB,
-                  t1 + (size_t)c0 * V, (unsigned)((c1 - c0) * RB), bar + s);
+                  t1 + (size_t)c0 * V, (unsigned)((c1 - c0) * RB), full + s);
     }
     if constexpr (MODE == kCheb)
-      bulk_load(st + sl.t0_off, t0 + (size_t)first * V, tile_bytes, bar + s);
+      bulk_load(st + sl.t0_off, t0 + (size_t)first * V, tile_bytes, full + s);
   };
 
   // This thread computes site l of every tile and the vectors of two 16-byte chunks of
@@ -314,23 +327,43 @@ __global__ void __launch_bounds__(kBlock, 2)
   int cc[Z] = {};
   double p = 0.0;
   float4 la = {}, lb = {};
-  if (mine > 0)
+  // Warps 0 .. kComputeWarps - 1 compute; thread kBlock (the next warp) issues the copies.
+  // A compute warp waits for a stage's full barrier and, once its lanes have read the
+  // stage, arrives on the stage's empty barrier; the producer refills a stage when all
+  // compute warps have arrived. No barrier spans the block inside the loop, and a wait
+  // that runs out ends the loop of that warp (uniformly: __any_sync) or of the producer.
+  const bool compute = threadIdx.x < kBlock;
+  if (threadIdx.x == kBlock) {
+    int issued = 0;
+    for (int jj = 0; jj < mine; ++jj) {
+      const int s = jj % S;
+      if (jj >= S && !mbar_wait(empty + s, (unsigned)(jj / S - 1) & 1u)) {
+        atomicOr(op.stage_err, 1u);
+        break;
+      }
+      fence_async_smem();
+      produce(jj);
+      issued = jj + 1;
+    }
+    // every copy issued has landed before the block leaves
+    for (int jj = issued > S ? issued - S : 0; jj < issued; ++jj)
+      mbar_wait(full + jj % S, (unsigned)(jj / S) & 1u);
+  }
+  if (compute && mine > 0)
     fetch(0, cc, p, la, lb);
-  if (threadIdx.x == 0)
-    for (int j = 0; j < S && j < mine; ++j)
-      produce(j);
-
-  int j = 0;
-  for (; j < mine; ++j) {
+  for (int j = 0; compute && j < mine; ++j) {
     int cn[Z] = {};
     double pn = 0.0;
     float4 lan = {}, lbn = {};
     if (j + 1 < mine)
       fetch(j + 1, cn, pn, lan, lbn);
     const int s = j % S;
-    const bool late = !mbar_wait(bar + s, (unsigned)(j / S) & 1u);
-    if (late)
-      atomicOr(op.stage_err, 1u);
+    const bool late = !mbar_wait(full + s, (unsigned)(j / S) & 1u);
+    if (__any_sync(0xffffffffu, late)) {
+      if (late)
+        atomicOr(op.stage_err, 1u);
+      break;
+    }
     const unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes + l * RB;
     const int i = ((int)blockIdx.x + j * G) * TS + l;
     if (F32 && i < n) {
@@ -455,25 +488,16 @@ __global__ void __launch_bounds__(kBlock, 2)
         }
       }
     }
-    // stage s is read: thread 0 may refill it; a wait that ran out ends the block's loop
-    if (__syncthreads_or(late))
-      break;
-    if (threadIdx.x == 0 && j + S < mine) {
-      fence_async_smem();
-      produce(j + S);
-    }
+    // this warp has read stage s
+    __syncwarp();
+    if ((threadIdx.x & 31) == 0)
+      mbar_arrive(empty + s);
 #pragma unroll
     for (int m = 0; m < Z; ++m)
       cc[m] = cn[m];
     p = pn;
     la = lan;
     lb = lbn;
-  }
-  if (j < mine && threadIdx.x == 0) {
-    // A wait ran out at tile j: the copies of tiles j .. j + S - 1 may still land in
-    // this block's shared memory; wait for each once more (bounded) before leaving.
-    for (int jj = j; jj < j + S && jj < mine; ++jj)
-      mbar_wait(bar + jj % S, (unsigned)(jj / S) & 1u);
   }
   // Slots in the order of even sites (chunk q, then chunk q + V/4) on every thread.
   if (sw) {
@@ -487,9 +511,9 @@ __global__ void __launch_bounds__(kBlock, 2)
     }
   }
   if constexpr (DOT == kDotLeft)
-    dot_finish_w<V, W>(re, im, dot, StageSlots<kHalf, 1>{});
+    dot_finish_w<V, W, StageSlots<kHalf, 1>, kComputeWarps>(re, im, dot, {});
   else if constexpr (DOT == kDotPair)
-    dot_finish_w<2 * V, 2 * W>(re, im, dot, StageSlots<kHalf, 2>{});
+    dot_finish_w<2 * V, 2 * W, StageSlots<kHalf, 2>, kComputeWarps>(re, im, dot, {});
 }
 
 // Stage layout for V vectors: the windows, then T_{k-2} and left as the launch needs them.
@@ -529,7 +553,7 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
                          const float2* t1, float2* out, const float2* left, const Dot& d)
 {
   auto* kernel = k_step_staged<V, Z, MODE, DOT, F32>;
-  const size_t smem = (size_t)sl.stages * sl.stage_bytes + kMaxStages * sizeof(uint64_t) +
+  const size_t smem = (size_t)sl.stages * sl.stage_bytes + 2 * kMaxStages * sizeof(uint64_t) +
                       (size_t)op.n_codes * (sizeof(double2) + sizeof(int2) + sizeof(float4));
   static std::mutex mu;
   static std::unordered_map<size_t, int> per_sm;  // blocks per SM by shared memory size
@@ -545,7 +569,7 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
     auto it = per_sm.find(smem);
     if (it == per_sm.end()) {
       int b = 0;
-      GQT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kBlock, smem));
+      GQT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kernel, kStageThreads, smem));
       it = per_sm.emplace(smem, b > 0 ? b : 1).first;
     }
     bps = it->second;
@@ -554,7 +578,7 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
   const int ntiles = (op.n + TS - 1) / TS;
   const int cap = device_info().sms * bps;
   const int grid = ntiles < cap ? ntiles : cap;
-  kernel<<<grid, kBlock, smem, stream()>>>(op, sl, t0, t1, out, left, d);
+  kernel<<<grid, kStageThreads, smem, stream()>>>(op, sl, t0, t1, out, left, d);
   count_launches(1);
   GQT_CUDA(cudaGetLastError());
   return GQT_OK;
@@ -600,10 +624,14 @@ bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, co
 {
   if (op.stage_nw <= 0 || !op.code || !op.stage_err || (mode != kApply && mode != kCheb))
     return false;
-  // automatic (0): the symmetric loop only. On B200 (graphene 2,097,152 sites, cubic
-  // 256^3; 16 FP32 vectors) its staged pair step was as fast or 41 % faster, while the
-  // staged direct step, at 16 warps per SM against the unstaged step's 32, was 9 % slower.
-  if (op.stage_stages < 0 || (op.stage_stages == 0 && dot != kDotPair && !f32))
+  // Automatic (0), from B200 measurements with 16 vectors on graphene 2,097,152 sites
+  // (rows of 3), square 1024^2 (rows of 4) and cubic 256^3 (rows of 6): the GQT_FP32R
+  // steps are always staged (their unstaged step ran 20-60 % slower); the GQT_FP32
+  // steps on rows of 6 only (direct 11 %, pair 11 % faster there; on rows of 3 and 4
+  // the unstaged steps, at 32 warps per SM, were as fast or 10-15 % faster).
+  if (op.stage_stages < 0)
+    return false;
+  if (op.stage_stages == 0 && !f32 && op.z < 6)
     return false;
   if (nvec != 16 && nvec != 32)
     return false;

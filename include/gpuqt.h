@@ -162,9 +162,9 @@ gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo);
  * ahead, and the block computes from shared memory. Entries whose offset lies in no
  * window (periodic wraps) gather from global memory. Every T_m is bit-identical to the
  * unstaged step's; moments agree to FP64 rounding (another summation order).
- * stages: -1 off; 0 automatic (the default): the symmetric loop (gqt_moments_doubled)
- * is staged and the direct loop is not, as measured fastest on B200; 1 both loops,
- * as many stages as fit; 2..4 both loops, that many stages.
+ * stages: -1 off; 0 automatic (the default), as measured fastest on B200: GQT_FP32R
+ * loops are staged, GQT_FP32 loops on rows of 6; 1 every loop, as many stages as fit;
+ * 2..4 every loop, that many stages.
  * gqt_ham_staging reports the setting and the windows (lo/hi: room for 8 ints each,
  * or null); windows 0 means the step is never staged for this operator. */
 gqt_status gqt_ham_set_staging(gqt_ham* h, int stages);

@@ -48,12 +48,16 @@ def test_staged_matches_unstaged(name, V):
     H.set_staging(-1)
     plain = g.moments(H, X, X, M)
     assert _rel(staged, plain) <= REL
-    H.set_staging(0)  # automatic: the direct loop is not staged
+    H.set_staging(0)  # automatic: staged on rows of 6 only
     auto = g.moments(H, X, X, M)
-    assert np.array_equal(auto[0], plain[0]) and np.array_equal(auto[1], plain[1])
+    if m.ell()["max_neighbor"] < 6:
+        assert np.array_equal(auto[0], plain[0]) and np.array_equal(auto[1], plain[1])
+    else:
+        assert _rel(auto, plain) <= REL
     if V <= 16:
+        H.set_staging(-1)
         plain_d = g.moments_doubled(H, X, M)
-        H.set_staging(0)  # automatic: the symmetric loop is staged
+        H.set_staging(0)  # automatic: staged on rows of 6 only
         assert _rel(g.moments_doubled(H, X, M), plain_d) <= REL
         H.set_staging(1)
         assert _rel(g.moments_doubled(H, X, M), plain_d) <= REL
