@@ -20,8 +20,9 @@ Also reported, on the same line:
   batch         the realisation batch (8 uneven square lattices, 64 vectors, FP32)
   cubic256      the 3D Anderson lattice 256^3 (z = 6): FP64 and 16-vector FP32 side by
                 side (DOS rate, one VAC and one MSD correlation step, errors)
-  precision     graphene 4M, 5000 moments: FP32-storage error against FP64 for the
-                DOS and 20 VAC steps (peak-relative and pointwise)
+  precision     graphene 4M, 5000 moments: error of the FP32, FP32X and FP32R forms
+                against FP64 for the DOS and 20 VAC steps (peak-relative and pointwise)
+  precision_msd graphene 2M, 3000 moments: the same for 20 MSD steps of 1 fs
   cpu_baseline  the reference's CPU path (oracle/_ref) on this host: one core, and
                 one process per core
 
@@ -447,9 +448,11 @@ def run_ours(args):
         if not args.no_cubic:
             cubic = measure_cubic(g, torch, tmp, stream, hbm_peak)
         precision = None
+        precision_msd = None
         if not args.no_precision:
             from gpuqt_b200 import precision_report
             precision = precision_report.report("graphene4m", 20)
+            precision_msd = precision_report.msd_report("graphene2m", 20)
         cpu = None
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             cpu = cpu_baseline_line(reference_dir(src, os.path.join(tmp, "ref")), n)
@@ -486,6 +489,7 @@ def run_ours(args):
                 "batch": batch,
                 "cubic256": cubic,
                 "precision": precision,
+                "precision_msd": precision_msd,
             }
             print(json.dumps(line), flush=True)
     finally:

@@ -75,6 +75,8 @@ _SIGS = {
     "gqt_ham_loop": (ctypes.c_int, [_vp, _ip, _ip, _ip]),
     "gqt_ham_set_staging": (ctypes.c_int, [_vp, ctypes.c_int]),
     "gqt_ham_staging": (ctypes.c_int, [_vp, _ip, _ip, _ip, _ip]),
+    "gqt_ham_stage_plan": (ctypes.c_int, [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _ip,
+                                          _ip]),
     "gqt_ham_create_batch": (ctypes.c_int, [ctypes.POINTER(EllDesc), ctypes.c_int,
                                             ctypes.POINTER(_vp)]),
     "gqt_ham_realisations": (ctypes.c_int, [_vp, _ip]),
@@ -402,10 +404,20 @@ class Hamiltonian:
         return w.value, c.value, k.value
 
     def set_staging(self, stages: int) -> None:
-        """Staged step of the FP32 moment loops: -1 off; 0 automatic (the default: the
-        symmetric loop is staged, the direct loop is not); 1 both loops, as many
-        shared-memory stages as fit; 2..4 both loops, that many (gqt_ham_set_staging)."""
+        """Staged step of the FP32 and FP32R moment loops: -1 off; 0 automatic (the
+        default: FP32R loops are staged, FP32 loops on rows of six); 1 every loop, as
+        many shared-memory stages as fit; 2..4 every loop, that many
+        (gqt_ham_set_staging)."""
         _call("gqt_ham_set_staging", self.h, int(stages))
+
+    def stage_plan(self, nvec: int, precision: int, symmetric: bool = False):
+        """(stages, windows) the staged step would use in a moment loop of nvec vectors
+        in `precision` under the current setting; (0, 0) when it is not staged
+        (gqt_ham_stage_plan)."""
+        s, w = ctypes.c_int(), ctypes.c_int()
+        _call("gqt_ham_stage_plan", self.h, int(nvec), int(precision), int(bool(symmetric)),
+              ctypes.byref(s), ctypes.byref(w))
+        return s.value, w.value
 
     @property
     def staging(self) -> tuple[int, list[tuple[int, int]]]:

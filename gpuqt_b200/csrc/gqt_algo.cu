@@ -1363,6 +1363,22 @@ extern "C" gqt_status gqt_ham_staging(const gqt_ham* h, int* stages, int* window
   return GQT_OK;
 }
 
+extern "C" gqt_status gqt_ham_stage_plan(const gqt_ham* h, int nvec, int precision,
+                                         int symmetric, int* stages, int* windows)
+{
+  if (!h || !stages)
+    return fail(GQT_ERR_ARG, "gqt_ham_stage_plan: null argument");
+  *stages = 0;
+  if (windows)
+    *windows = 0;
+  if (precision != GQT_FP32 && precision != GQT_FP32R)
+    return GQT_OK;
+  const Op op = make_op(h, nvec);
+  *stages = stage_plan(op, nvec, symmetric ? kDotPair : kDotLeft, precision == GQT_FP32R,
+                       windows);
+  return GQT_OK;
+}
+
 // ------------------------------------------------------------------ autotuner
 extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_moments,
                                         const int* candidates, int n_candidates, int* best,

@@ -95,7 +95,7 @@ const FormOps* forms_fp64(int nvec);
 const FormOps* forms_fp32(int nvec);
 // GQT_FP32X: moment loops only (dot, step, step_pair; nvec 1, 4, 16).
 const FormOps* forms_fp32x(int nvec);
-// GQT_FP32R (gqt_stage.cu): moment loops only (dot, step, step_pair; nvec 16 and 32).
+// GQT_FP32R (gqt_stage.cu): moment loops only (dot, step, step_pair; nvec 4, 16 and 32).
 const FormOps* forms_fp32r(int nvec);
 // src (GQT_FP64 or GQT_FP32 storage, `total` elements) into FP32X storage at dst.
 gqt_status convert_to_x(size_t total, int from, const void* src, void* dst, uintptr_t xlo);
@@ -124,6 +124,10 @@ bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, co
 gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
                       const void* t1, void* out, const void* left, const Dot& d,
                       bool f32 = false);
+// The stages and windows (*windows) the staged Chebyshev step of a moment loop would use
+// for nvec vectors (dot kDotLeft: direct, kDotPair: symmetric sets); 0 when it would not
+// be staged.
+int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows);
 // Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
 // at the number of blocks that are resident at once on all SMs.
 int grid_for(const void* kernel, size_t total);

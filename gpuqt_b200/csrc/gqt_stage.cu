@@ -132,10 +132,11 @@ struct StageSlots {
 // potential multiplied by RN(1 / E_max) in FP64) is kept as two FP32 parts, hi =
 // RN_fp32(a) and lo = RN_fp32(a - hi), so that it is not perturbed at FP32 precision (a
 // fixed perturbation of H shifts the spectrum, and its error grows linearly with the
-// moment index); T_k = 2 (H / E_max) T_{k-1} - T_{k-2} is summed with FP32 fused
-// multiply-adds, the hi products and the lo products in two accumulators (neighbours in
-// ELL order) added once per element. The moments are summed in FP64 from the stored
-// FP32 values (the product of two FP32 values is exact in FP64).
+// moment index); (H / E_max) T_{k-1} is summed with FP32 fused multiply-adds, the hi
+// products and the lo products in two accumulators (neighbours in ELL order), and T_k =
+// 2 (hi + lo) - T_{k-2} is formed with one rounding of the hi part (cheb_part). The
+// moments are summed in FP64 from the stored FP32 values (the product of two FP32
+// values is exact in FP64).
 __device__ __forceinline__ float2 split_f32(double a)
 {
   const float hi = (float)a;
@@ -173,15 +174,30 @@ __device__ __forceinline__ void cmac_f32(AccF32& a, float4 h, float2 y)
   a.il = fmaf(h.w, y.x, a.il);
 }
 
+// One part of T_k = 2 (hi + lo) - T_{k-2} with a single rounding of the hi sum: 2 hi -
+// T_{k-2} is split exactly into s + e (Knuth's TwoSum; 2 hi is exact), then 2 lo and e
+// are added to s. Rounding hi + lo first leaves an error of the order of hi's last
+// place, and hi is near T_{k-2} / 2 where T_k is small: in a model of the recurrence
+// (graphene, 2000 moments) that rounding gave 14x the moment error of this form, 23x that
+// of the FP32 form. Explicit round-to-nearest intrinsics keep the compiler from fusing
+// the sequence.
+__device__ __forceinline__ float cheb_part(float hi, float lo, float y0)
+{
+  const float s = __fmaf_rn(2.0f, hi, -y0);
+  const float a1 = __fadd_rn(s, y0);      // the part of s from 2 hi
+  const float b1 = __fsub_rn(s, a1);      // the part of s from -T_{k-2}
+  const float e = __fadd_rn(__fmaf_rn(2.0f, hi, -a1), __fsub_rn(-y0, b1));
+  return __fadd_rn(s, __fmaf_rn(2.0f, lo, e));
+}
+
 // T_k = 2 acc - T_{k-2} (kCheb), or acc (kApply)
 template <int MODE>
 __device__ __forceinline__ float2 acc_finish(const AccF32& a, float2 y0)
 {
-  const float r = a.r + a.rl, i = a.i + a.il;
   if constexpr (MODE == kCheb)
-    return make_float2(fmaf(2.0f, r, -y0.x), fmaf(2.0f, i, -y0.y));
+    return make_float2(cheb_part(a.r, a.rl, y0.x), cheb_part(a.i, a.il, y0.y));
   else
-    return make_float2(r, i);
+    return make_float2(a.r + a.rl, a.i + a.il);
 }
 
 template <int V, int Z, int MODE, int DOT, bool F32>
@@ -516,12 +532,13 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     dot_finish_w<2 * V, 2 * W, StageSlots<kHalf, 2>, kComputeWarps>(re, im, dot, {});
 }
 
-// Stage layout for V vectors: the windows, then T_{k-2} and left as the launch needs them.
-bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayout& sl)
+// Stage layout for V vectors over the first nw windows: the windows, then T_{k-2} as
+// the launch needs it; true when at least two stages of it fit.
+bool stage_layout_nw(const Op& op, int V, int mode, int nw, int stages, StageLayout& sl)
 {
   const int TS = kBlock * kStageW / V, RB = V * (int)sizeof(float2);
   sl = StageLayout{};
-  sl.nw = op.stage_nw;
+  sl.nw = nw;
   int off = 0;
   for (int w = 0; w < sl.nw; ++w) {
     sl.win_lo[w] = op.stage_lo[w];
@@ -546,6 +563,18 @@ bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayou
   stages = stages > fit ? fit : stages;
   sl.stages = stages > kMaxStages ? kMaxStages : stages;
   return sl.nw > 0 && sl.stages >= 2;
+}
+
+// The windows come most used first (after the one holding offset 0); when two stages of
+// all of them do not fit, the last ones are left out (their entries gather from global
+// memory) until two do.
+bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayout& sl)
+{
+  (void)dot;  // left never takes shared memory: both moment modes share the layout
+  for (int nw = op.stage_nw; nw >= 1; --nw)
+    if (stage_layout_nw(op, V, mode, nw, stages, sl))
+      return true;
+  return false;
 }
 
 template <int V, int Z, int MODE, int DOT, bool F32>
@@ -619,8 +648,9 @@ gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, cons
 
 }  // namespace
 
-bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
-                   const void* left, bool f32)
+// Whether the staged step serves a step of this operator, vector count and mode, and
+// its layout (the vectors' alignment aside).
+static bool stage_fits(const Op& op, int nvec, int mode, int dot, bool f32, StageLayout& sl)
 {
   if (op.stage_nw <= 0 || !op.code || !op.stage_err || (mode != kApply && mode != kCheb))
     return false;
@@ -641,12 +671,27 @@ bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, co
     return false;
   if (op.z != 3 && op.z != 4 && op.z != 6)
     return false;
+  return stage_layout(op, nvec, mode, dot, op.stage_stages, sl);
+}
+
+bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
+                   const void* left, bool f32)
+{
   // bulk copies start on 16-byte boundaries (rows are nvec * 8 >= 32 bytes)
   auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
   if (!aligned(t1) || (mode == kCheb && !aligned(t0)) || (dot == kDotLeft && !aligned(left)))
     return false;
   StageLayout sl;
-  return stage_layout(op, nvec, mode, dot, op.stage_stages, sl);
+  return stage_fits(op, nvec, mode, dot, f32, sl);
+}
+
+int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows)
+{
+  StageLayout sl;
+  const bool on = stage_fits(op, nvec, kCheb, dot, f32, sl);
+  if (windows)
+    *windows = on ? sl.nw : 0;
+  return on ? sl.stages : 0;
 }
 
 gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
@@ -828,6 +873,8 @@ const FormOps* table_r()
 const FormOps* forms_fp32r(int nvec)
 {
   switch (nvec) {
+    case 4:
+      return table_r<4>();
     case 16:
       return table_r<16>();
     case 32:

@@ -52,10 +52,11 @@ enum {
    * few 1e-6 at late VAC times. Vectors of this form cannot be created. */
   GQT_FP32X = 2,
   /* No counterpart in the reference. A form of the moment recurrence only (as
-   * GQT_FP32X; 16 or 32 vectors per launch): FP32 vectors and FP32 hoppings (divided
-   * by energy_max in FP64, then rounded once), the Chebyshev recurrence in FP32, and
-   * the moments summed in FP64 from the stored FP32 values. Runs on GQT_FP32 vectors
-   * as they are, or on FP32 copies of GQT_FP64 ones. */
+   * GQT_FP32X; 4, 16 or 32 vectors per launch): FP32 vectors and FP32 hoppings (each
+   * hopping and potential divided by energy_max in FP64, then held as two FP32 parts,
+   * hi = RN(a) and lo = RN(a - hi)), the Chebyshev recurrence in FP32, and the moments
+   * summed in FP64 from the stored FP32 values. Runs on GQT_FP32 vectors as they are,
+   * or on FP32 copies of GQT_FP64 ones. */
   GQT_FP32R = 3
 };
 
@@ -154,14 +155,16 @@ gqt_status gqt_ham_batch_tile(const gqt_ham* h, int* tile_sites);
 gqt_status gqt_ham_set_loop(gqt_ham* h, int window, int chunk_sites);
 gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo);
 
-/* The staged step of the GQT_FP32 moment loops (no counterpart in the reference) over
- * the coded operator, for 16 or 32 vectors and rows of 3, 4 or 6 entries. The sites are
- * cut into tiles; per tile, one thread copies the rows of T_{k-1} its gathers read (a
- * few windows of frequent neighbour offsets, found at upload), its T_{k-2} rows and
- * its left rows into shared memory with bulk asynchronous copies, several tiles
- * ahead, and the block computes from shared memory. Entries whose offset lies in no
- * window (periodic wraps) gather from global memory. Every T_m is bit-identical to the
- * unstaged step's; moments agree to FP64 rounding (another summation order).
+/* The staged step of the GQT_FP32 and GQT_FP32R moment loops (no counterpart in the
+ * reference) over the coded operator, for 16 or 32 vectors and rows of 3, 4 or 6
+ * entries. The sites are cut into tiles; per tile, one thread copies the rows of
+ * T_{k-1} its gathers read (a few windows of frequent neighbour offsets, found at
+ * upload) and its T_{k-2} rows into shared memory with bulk asynchronous copies,
+ * several tiles ahead, and the block computes from shared memory (left is read into
+ * registers). Entries whose offset lies in no window (periodic wraps, and the least
+ * used windows when two stages of all do not fit) gather from global memory. Every
+ * T_m is bit-identical to the unstaged step's; moments agree to FP64 rounding (another
+ * summation order).
  * stages: -1 off; 0 automatic (the default), as measured fastest on B200: GQT_FP32R
  * loops are staged, GQT_FP32 loops on rows of 6; 1 every loop, as many stages as fit;
  * 2..4 every loop, that many stages.
@@ -169,6 +172,12 @@ gqt_status gqt_ham_loop(const gqt_ham* h, int* window, int* chunks, int* halo);
  * or null); windows 0 means the step is never staged for this operator. */
 gqt_status gqt_ham_set_staging(gqt_ham* h, int stages);
 gqt_status gqt_ham_staging(const gqt_ham* h, int* stages, int* windows, int* lo, int* hi);
+/* The stages and windows the staged step would use in a moment loop of nvec vectors in
+ * `precision` (GQT_FP32 or GQT_FP32R; symmetric != 0: the loop of symmetric moment
+ * sets) under the current setting; *stages = 0 when that loop is not staged. No
+ * counterpart in the reference. */
+gqt_status gqt_ham_stage_plan(const gqt_ham* h, int nvec, int precision, int symmetric,
+                              int* stages, int* windows);
 gqt_status gqt_ham_realisations(const gqt_ham* h, int* count);
 gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
                                double* energy_max);

@@ -86,7 +86,7 @@ def test_fp32x_doubled_matches_fp64(nvec):
 
 @pytest.mark.slow
 def test_fp32x_graphene4m_dos_and_20_vac_steps():
-    r = P.report("graphene4m", vac_steps=20)
+    r = P.report("graphene4m", vac_steps=20, fp32r=False)
     x = r["fp32x"]
     for q in ("dos", "vac"):
         assert x[q]["energy_rel_in_band_max"] <= 1e-6, (q, x[q])

@@ -14,6 +14,7 @@ import pytest
 
 import gpuqt_b200 as g
 from conftest import fixture_dir
+from gpuqt_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
 
@@ -107,3 +108,29 @@ def test_staging_arguments():
     ell = g.moments(H, X, X, 50)  # the ELL arrays are never staged
     H.set_format(g.FORMAT_CODED)
     assert _rel(g.moments(H, X, X, 50), ell) <= REL
+
+
+def test_stage_plan_leaves_out_windows_that_do_not_fit(tmp_path):
+    """cubic 8 x 64 x 64: the periodic wraps along the short axis are taken by 1/8 of the
+    entries, so the upload finds more windows than two stages of them fit in shared
+    memory. The least used windows are left out (their entries gather from global
+    memory) and the step stays staged, with the same moments as the unstaged step."""
+    d = W.write_input_dir(str(tmp_path / "cubic"), "cubic", (8, 64, 64), anderson=16.5,
+                          energy_max=15.0, moments=120, calculate=(), seed=13)
+    m = g.Model.load(d)
+    H = g.Hamiltonian(m)
+    _, wins = H.staging
+    V, M = 16, 120
+    for prec in (g.FP32, g.FP32R):
+        stages, used = H.stage_plan(V, prec)
+        assert stages >= 2 and 1 <= used < len(wins), (prec, stages, used, wins)
+        assert H.stage_plan(V, prec, symmetric=True)[0] >= 2
+    assert H.stage_plan(V, g.FP64) == (0, 0)
+    X = g.Vector.from_host(*_states(m, V), nvec=V, precision=g.FP32)
+    staged = {p: g.moments(H, X, X, M, precision=p) for p in (g.FP32, g.FP32R)}
+    staged_d = g.moments_doubled(H, X, M, precision=g.FP32R)
+    H.set_staging(-1)
+    assert H.stage_plan(V, g.FP32R) == (0, 0)
+    for p in (g.FP32, g.FP32R):
+        assert _rel(staged[p], g.moments(H, X, X, M, precision=p)) <= REL
+    assert _rel(staged_d, g.moments_doubled(H, X, M, precision=g.FP32R)) <= REL
