@@ -965,6 +965,54 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
     X.upload(*B.scatter(per0))
     q32, j32 = g.moments_doubled(B, X, moments)
     dbl_err = dos_error(g, m0, (r64, i64), (q32[0, 0], j32[0, 0]))
+    del X, mu
+
+    # The FP32R form (FP32 recurrence, the staged batch step with each model's windows):
+    # 32 vectors per launch direct, 16 for symmetric sets; the same vectors and checks.
+    def fp32r(Vr, doubled):
+        Xr = g.Vector(B.n, nvec=Vr, precision=g.FP32)
+        mur = torch.empty(2 * moments * len(models) * Vr, dtype=torch.float64, device="cuda")
+        if doubled:
+            run = lambda: g.moments_doubled_device(B, Xr, moments, mur.data_ptr(),
+                                                   precision=g.FP32R)
+        else:
+            run = lambda: g.moments_device(B, Xr, Xr, moments, mur.data_ptr(),
+                                           precision=g.FP32R)
+        Xr.upload(*B.scatter([(p[0][:Vr], p[1][:Vr]) for p in per0]))
+        run()
+        torch.cuda.synchronize()
+        ms = 0.0
+        for k in range(vectors // Vr):
+            per = []
+            for m in models:
+                ph = rng.uniform(0.0, 2 * np.pi, size=(Vr, m.n))
+                per.append((np.cos(ph), np.sin(ph)))
+            Xr.upload(*B.scatter(per))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            run()
+            b.record(stream)
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+        r = vectors * sites * moments / (ms / 1e3)
+        Xr.upload(*B.scatter([(p[0][:Vr], p[1][:Vr]) for p in per0]))
+        if doubled:
+            qr, qi = g.moments_doubled(B, Xr, moments, precision=g.FP32R)
+            bps = fp32_pair_bytes_per_site_vector_step(Vr, z=4) * B.n / sites
+            ach = r / 2 * bps / 1e9
+        else:
+            qr, qi = g.moments(B, Xr, Xr, moments, precision=g.FP32R)
+            bps = fp32_bytes_per_site_vector(Vr, z=4) * B.n / sites
+            ach = r * bps / 1e9
+        stages, slots = B.stage_plan(Vr, g.FP32R, symmetric=doubled)
+        return {"site_moments_per_s": r, "vectors_per_launch": Vr, "ms_total": ms,
+                "bytes_per_site_moment" if not doubled else "bytes_per_site_step": bps,
+                "achieved_gbs": ach, "frac": ach / hbm_peak,
+                "dos_err_vs_fp64": dos_error(g, m0, (r64, i64), (qr[0, 0], qi[0, 0])),
+                "stages": stages, "window_slots": slots}
+
+    fp32r_direct = fp32r(32, False) if B.format == g.FORMAT_CODED else None
+    fp32r_doubled = fp32r(16, True) if B.format == g.FORMAT_CODED else None
     return {"realisations": [[m.n, round(m.energy_max, 4)] for m in models],
             "doubled": {"site_moments_per_s": vectors * sites * moments / (dbl_ms / 1e3),
                         "ms_total": dbl_ms, "dos_err_vs_fp64": dbl_err},
@@ -975,7 +1023,8 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
             "site_moments_per_s": rate, "ms_total": total_ms,
             "achieved_gbs": rate * bytes_site_moment / 1e9,
             "frac": rate * bytes_site_moment / 1e9 / hbm_peak,
-            "dos_err_vs_fp64": err}
+            "dos_err_vs_fp64": err,
+            "fp32r": fp32r_direct, "fp32r_doubled": fp32r_doubled}
 
 
 def main():

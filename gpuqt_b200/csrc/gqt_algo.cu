@@ -146,6 +146,17 @@ Op make_op(const gqt_ham* h, int nvec = 1)
       op.stage_hi[w] = h->stage_hi[w];
     }
     op.stage_err = h->stage_err;
+  } else if (h->use_codes && h->n_real > 1 && h->stage_rtab && h->stage_rnw > 0 &&
+             h->stage_err) {
+    // realisation batch: common slots, each model's windows in the device table
+    op.stage_nw = h->stage_rnw;
+    op.stage_stages = h->stage_stages;
+    for (int w = 0; w < h->stage_rnw; ++w) {
+      op.stage_lo[w] = 0;
+      op.stage_hi[w] = h->stage_rwidth[w];
+    }
+    op.stage_err = h->stage_err;
+    op.stage_rtab = h->stage_rtab;
   }
   return op;
 }
@@ -1020,8 +1031,6 @@ static gqt_status moments_form_run(const gqt_ham* h, const gqt_vec* left, const 
   // GQT_FP32R stores its vectors as GQT_FP32 does: FP32 vectors run as they are.
   const int store = precision == GQT_FP32R ? GQT_FP32 : precision;
   if (precision == GQT_FP32R) {
-    if (h->n_real > 1)
-      return fail(GQT_ERR_STATE, "%s: the FP32R form runs on one model, not a batch", w);
     if (right->precision == GQT_FP32X || left->precision == GQT_FP32X ||
         right->precision == GQT_FP32R || left->precision == GQT_FP32R)
       return fail(GQT_ERR_ARG, "%s: the FP32R form reads FP32 or FP64 vectors", w);
@@ -1375,7 +1384,7 @@ extern "C" gqt_status gqt_ham_stage_plan(const gqt_ham* h, int nvec, int precisi
     return GQT_OK;
   const Op op = make_op(h, nvec);
   *stages = stage_plan(op, nvec, symmetric ? kDotPair : kDotLeft, precision == GQT_FP32R,
-                       windows);
+                       windows, h->n_real);
   return GQT_OK;
 }
 

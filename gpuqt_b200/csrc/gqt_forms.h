@@ -127,7 +127,7 @@ gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
 // The stages and windows (*windows) the staged Chebyshev step of a moment loop would use
 // for nvec vectors (dot kDotLeft: direct, kDotPair: symmetric sets); 0 when it would not
 // be staged.
-int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows);
+int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows, int R = 1);
 // Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
 // at the number of blocks that are resident at once on all SMs.
 int grid_for(const void* kernel, size_t total);

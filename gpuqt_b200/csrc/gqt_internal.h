@@ -122,6 +122,13 @@ struct gqt_ham {
   int stage_lo[8] = {}, stage_hi[8] = {};
   int stage_stages = 0;
   unsigned* stage_err = nullptr;
+  // Realisation batches: each model's own windows in stage_rnw common slots (slot w is
+  // stage_rwidth[w] + 1 offsets wide, the widest of the models' w-th windows). Device
+  // table: [n_real][8] window lo, [n_real] windows of the model, [n_real][n_codes] the
+  // slot holding each code's offset for that model (-1: gathered from global memory).
+  int stage_rnw = 0;
+  int stage_rwidth[8] = {};
+  int* stage_rtab = nullptr;
   std::unique_ptr<gqt::Workspace> ws;
   ~gqt_ham();
 };

@@ -62,6 +62,9 @@ struct Op {
   int stage_lo[kStageWin];
   int stage_hi[kStageWin];
   unsigned* stage_err;
+  // Realisation batches (null for one model): gqt_ham::stage_rtab; the slots are then
+  // stage_lo[w] = 0, stage_hi[w] = the slot's width.
+  const int* __restrict__ stage_rtab;
 };
 
 struct Dot {

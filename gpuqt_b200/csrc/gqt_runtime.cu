@@ -441,6 +441,7 @@ gqt_ham::~gqt_ham()
   cudaFree(code_hop);
   cudaFree(code_xx);
   cudaFree(stage_err);
+  cudaFree(stage_rtab);
 }
 
 namespace {
@@ -701,47 +702,30 @@ bool is_hermitian(const Packed& P)
 }
 
 // Windows of the staged FP32 step (gqt_stage.cu): the neighbour offsets j - i taken by
-// at least n / 64 entries, and offset 0, grouped where consecutive offsets lie at most
+// at least rows / 64 entries, and offset 0, grouped where consecutive offsets lie at most
 // 16 rows apart; the group holding 0 first, then the most used, at most 8 in all. A
 // tile of the step copies each window's rows into shared memory; entries whose offset
 // lies in no window (periodic wraps, taken by a few rows per lattice line) gather from
 // global memory.
-void plan_stage_windows(const Packed& P, const std::vector<uint8_t>& codes,
-                        const std::vector<int>& delta, gqt_ham* h)
+struct StageWin {
+  int lo, hi;
+  long long use;
+};
+
+std::vector<StageWin> group_windows(const std::map<int, long long>& use, long long rows)
 {
-  static_assert(sizeof(h->stage_lo) / sizeof(int) == kStageWin, "window table size");
-  const size_t nc = delta.size();
-  std::vector<std::vector<long long>> part(16, std::vector<long long>(nc, 0));
-  parallel_rows(P.n, [&](long long lo, long long hi, int chunk) {
-    auto& u = part[chunk];
-    for (int m = 0; m < P.z; ++m)
-      for (long long i = lo; i < hi; ++i)
-        ++u[codes[(size_t)m * P.n + i]];
-  });
-  std::map<int, long long> use;  // offset -> entries
-  use[0] += 0;
-  for (size_t c = 0; c < nc; ++c) {
-    long long u = 0;
-    for (auto& p : part)
-      u += p[c];
-    use[delta[c]] += u;
-  }
-  struct Win {
-    int lo, hi;
-    long long use;
-  };
-  std::vector<Win> wins;
+  std::vector<StageWin> wins;
   for (const auto& [d, u] : use) {
-    if (d != 0 && u < (long long)P.n / 64)
+    if (d != 0 && u < rows / 64)
       continue;
     if (!wins.empty() && (long long)d - wins.back().hi <= 16) {
       wins.back().hi = d;
       wins.back().use += u;
     } else {
-      wins.push_back(Win{d, d, u});
+      wins.push_back(StageWin{d, d, u});
     }
   }
-  std::stable_sort(wins.begin(), wins.end(), [](const Win& a, const Win& b) {
+  std::stable_sort(wins.begin(), wins.end(), [](const StageWin& a, const StageWin& b) {
     const bool za = a.lo <= 0 && a.hi >= 0, zb = b.lo <= 0 && b.hi >= 0;
     if (za != zb)
       return za;
@@ -749,6 +733,37 @@ void plan_stage_windows(const Packed& P, const std::vector<uint8_t>& codes,
   });
   if (wins.size() > (size_t)kStageWin)
     wins.resize(kStageWin);
+  return wins;
+}
+
+// Entries per code over the rows [lo, hi).
+std::vector<long long> code_use(const Packed& P, const std::vector<uint8_t>& codes, size_t nc,
+                                long long lo, long long hi)
+{
+  std::vector<std::vector<long long>> part(16, std::vector<long long>(nc, 0));
+  parallel_rows(hi - lo, [&](long long a, long long b, int chunk) {
+    auto& u = part[chunk];
+    for (int m = 0; m < P.z; ++m)
+      for (long long i = lo + a; i < lo + b; ++i)
+        ++u[codes[(size_t)m * P.n + i]];
+  });
+  std::vector<long long> use(nc, 0);
+  for (auto& p : part)
+    for (size_t c = 0; c < nc; ++c)
+      use[c] += p[c];
+  return use;
+}
+
+void plan_stage_windows(const Packed& P, const std::vector<uint8_t>& codes,
+                        const std::vector<int>& delta, gqt_ham* h)
+{
+  static_assert(sizeof(h->stage_lo) / sizeof(int) == kStageWin, "window table size");
+  const std::vector<long long> per_code = code_use(P, codes, delta.size(), 0, P.n);
+  std::map<int, long long> use;  // offset -> entries
+  use[0] += 0;
+  for (size_t c = 0; c < delta.size(); ++c)
+    use[delta[c]] += per_code[c];
+  const std::vector<StageWin> wins = group_windows(use, P.n);
   h->stage_nw = (int)wins.size();
   for (size_t w = 0; w < wins.size(); ++w) {
     h->stage_lo[w] = wins[w].lo;
@@ -756,7 +771,59 @@ void plan_stage_windows(const Packed& P, const std::vector<uint8_t>& codes,
   }
 }
 
-gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h)
+// The same per model of a realisation batch (rows [offset[r], offset[r] + n[r])), in
+// common slots: slot w holds model r's w-th window, as wide as the widest of them. The
+// device table gives the kernel each model's window starts and, per (model, code), the
+// slot whose rows hold the code's neighbours (-1 when the model's windows miss it).
+gqt_status plan_stage_windows_batch(const Packed& P, const std::vector<uint8_t>& codes,
+                                    const std::vector<int>& delta,
+                                    const std::vector<int>& offset,
+                                    const std::vector<int>& n, gqt_ham* h)
+{
+  const int R = (int)n.size();
+  const size_t nc = delta.size();
+  std::vector<int> tab((size_t)R * (kStageWin + 1 + nc), 0);
+  int* lo = tab.data();
+  int* nw = lo + (size_t)R * kStageWin;
+  int* slot = nw + R;
+  int slots = 0;
+  int width[kStageWin] = {};
+  for (int r = 0; r < R; ++r) {
+    const std::vector<long long> per_code = code_use(P, codes, nc, offset[r], offset[r] + n[r]);
+    std::map<int, long long> use;
+    use[0] += 0;
+    for (size_t c = 0; c < nc; ++c)
+      if (per_code[c] > 0)
+        use[delta[c]] += per_code[c];
+    const std::vector<StageWin> wins = group_windows(use, n[r]);
+    nw[r] = (int)wins.size();
+    slots = nw[r] > slots ? nw[r] : slots;
+    for (int w = 0; w < nw[r]; ++w) {
+      lo[(size_t)r * kStageWin + w] = wins[w].lo;
+      width[w] = std::max(width[w], wins[w].hi - wins[w].lo);
+    }
+    for (size_t c = 0; c < nc; ++c) {
+      int s = -1;
+      for (int w = 0; w < nw[r] && s < 0; ++w)
+        if (per_code[c] > 0 && delta[c] >= wins[w].lo && delta[c] <= wins[w].hi)
+          s = w;
+      slot[(size_t)r * nc + c] = s;
+    }
+  }
+  h->stage_rnw = slots;
+  for (int w = 0; w < kStageWin; ++w)
+    h->stage_rwidth[w] = width[w];
+  GQT_CUDA(cudaMalloc(&h->stage_rtab, tab.size() * sizeof(int)));
+  GQT_CUDA(cudaMemcpy(h->stage_rtab, tab.data(), tab.size() * sizeof(int),
+                      cudaMemcpyHostToDevice));
+  return GQT_OK;
+}
+
+// batch_offset / batch_n: the models of a realisation batch (their staging windows are
+// planned per model), or null for one model.
+gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ham* h,
+                         const std::vector<int>* batch_offset = nullptr,
+                         const std::vector<int>* batch_n = nullptr)
 {
   const size_t pairs = (size_t)P.n * P.z;
   h->n = P.n;
@@ -794,7 +861,10 @@ gqt_status upload_packed(const Packed& P, double energy_max, bool has_xx, gqt_ha
     GQT_CUDA(cudaMemcpy(h->code_xx, cxx.data(), nc * sizeof(double), cudaMemcpyHostToDevice));
     h->n_codes = (int)nc;
     h->use_codes = 1;
-    plan_stage_windows(P, codes, delta, h);
+    if (batch_offset)
+      GQT_TRY(plan_stage_windows_batch(P, codes, delta, *batch_offset, *batch_n, h));
+    else
+      plan_stage_windows(P, codes, delta, h);
     GQT_CUDA(cudaMalloc(&h->stage_err, sizeof(unsigned)));
     GQT_CUDA(cudaMemset(h->stage_err, 0, sizeof(unsigned)));
   }
@@ -862,7 +932,10 @@ extern "C" gqt_status gqt_ham_create_batch(const gqt_ell_desc* descs, int count,
   for (int r = 0; r < count; ++r)
     has_xx = has_xx && descs[r].xx != nullptr;
   // Each model is pre-divided by its own E_max, so the operator is applied with 1.
-  GQT_TRY(upload_packed(P, 1.0, has_xx, h));
+  std::vector<int> real_n(count);
+  for (int r = 0; r < count; ++r)
+    real_n[r] = descs[r].n;
+  GQT_TRY(upload_packed(P, 1.0, has_xx, h, &offset, &real_n));
   h->n_real = count;
   h->real_offset = offset;
   for (int r = 0; r < count; ++r) {

@@ -200,10 +200,16 @@ __device__ __forceinline__ float2 acc_finish(const AccF32& a, float2 y0)
     return make_float2(a.r + a.rl, a.i + a.il);
 }
 
-template <int V, int Z, int MODE, int DOT, bool F32>
+// MULTI: one step of a realisation batch (op.stage_rtab: each model's windows; md: the
+// models' tiles and the per-block, per-model sum slots that k_tile_reduce combines).
+// Tiles never straddle two models (every model is padded to 1024 sites). A block's
+// tiles come in increasing order, so the models it meets are consecutive runs: when the
+// next tile is in another model, the compute warps reduce their sums over the block
+// (a named barrier of the compute warps only) and write the block's slot of the model.
+template <int V, int Z, int MODE, int DOT, bool F32, bool MULTI = false>
 __global__ void __launch_bounds__(kStageThreads, 2)
   k_step_staged(Op op, StageLayout sl, const float2* t0, const float2* __restrict__ t1,
-                float2* out, const float2* __restrict__ left, Dot dot)
+                float2* out, const float2* __restrict__ left, Dot dot, MultiDot md)
 {
   using A = FastArith;
   constexpr int W = kStageW;
@@ -219,22 +225,51 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   double2* hop = reinterpret_cast<double2*>(empty + kMaxStages);
   // GQT_FP32R: the hoppings divided by E_max as FP32 (hi, lo) parts
   float4* hopf = reinterpret_cast<float4*>(hop + op.n_codes);
-  // per code: byte offset in a stage of site 0's neighbour row (-1: gathered from
-  // global memory), and the offset j - i
+  // per code (MULTI: per model and code): byte offset in a stage of site 0's neighbour
+  // row (-1: gathered from global memory), and the offset j - i
   int2* cinfo = reinterpret_cast<int2*>(hopf + op.n_codes);
+  // MULTI: md's fields as values (lambdas then capture no kernel parameter by address)
+  const int R = MULTI ? md.n_real : 1;
+  const int* const tile_first = md.tile_first;
+  const long long tile_sites = md.tile_sites;
+  double* const partials = md.partials;
+  // MULTI: each model's window starts [R][kStageWin], then its window count [R]
+  int* rlo = reinterpret_cast<int*>(cinfo + (size_t)R * op.n_codes);
+  const int* rnw = rlo + R * kStageWin;
+  __shared__ int abort_flag;  // MULTI: a wait ran out; the block computes no further
 
   for (int c = threadIdx.x; c < op.n_codes; c += blockDim.x) {
     hop[c] = op.code_hop[c];
     hopf[c] = scaled_hop(op.code_hop[c], op);
-    const int d = op.code_delta[c];
-    int o = -1;
+    if constexpr (!MULTI) {
+      const int d = op.code_delta[c];
+      int o = -1;
 #pragma unroll
-    for (int w = 0; w < kStageWin; ++w)
-      if (w < sl.nw && o < 0 && d >= sl.win_lo[w] && d <= sl.win_lo[w] + sl.win_rows[w] - TS)
-        o = sl.win_off[w] + (d - sl.win_lo[w]) * RB;
-    cinfo[c] = make_int2(o, d);
+      for (int w = 0; w < kStageWin; ++w)
+        if (w < sl.nw && o < 0 && d >= sl.win_lo[w] && d <= sl.win_lo[w] + sl.win_rows[w] - TS)
+          o = sl.win_off[w] + (d - sl.win_lo[w]) * RB;
+      cinfo[c] = make_int2(o, d);
+    }
+  }
+  if constexpr (MULTI) {
+    const int* tab = op.stage_rtab;
+    for (int k = threadIdx.x; k < R * (kStageWin + 1); k += blockDim.x)
+      rlo[k] = tab[k];
+    const int* slot = tab + R * (kStageWin + 1);
+    for (int k = threadIdx.x; k < R * op.n_codes; k += blockDim.x) {
+      const int r = k / op.n_codes, d = op.code_delta[k % op.n_codes], w = slot[k];
+      // the planner put d inside model r's window w, which its slot is wide enough for
+      // (constant indices into sl: a runtime one would copy it to local memory)
+      int o = -1;
+#pragma unroll
+      for (int q = 0; q < kStageWin; ++q)
+        if (q == w && q < sl.nw)
+          o = sl.win_off[q] + (d - tab[r * kStageWin + q]) * RB;
+      cinfo[k] = make_int2(o, d);
+    }
   }
   if (threadIdx.x == 0) {
+    abort_flag = 0;
     for (int s = 0; s < S; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, kComputeWarps);
@@ -250,6 +285,13 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   const int mine = (int)blockIdx.x < ntiles ? (ntiles - 1 - (int)blockIdx.x) / G + 1 : 0;
   // the site's own row (offset 0, in window 0)
   const int xofs = sl.win_off[0] - sl.win_lo[0] * RB;
+  // MULTI: the model of this block's tile j (tiles come in increasing order)
+  int rp = 0;
+  auto model_of = [&](int j, int& r) {
+    const long long first = (long long)((int)blockIdx.x + j * G) * TS;
+    while (r + 1 < R && first >= (long long)tile_first[r + 1] * tile_sites)
+      ++r;
+  };
 
   // Thread 0: the copies of this block's tile j into stage j % S.
   auto produce = [&](int j) {
@@ -257,9 +299,21 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes;
     const long long first = (long long)((int)blockIdx.x + j * G) * TS;
     const long long last = first + TS < n ? first + TS : n;
+    int wlo[kStageWin];  // window starts (MULTI: the tile's model's)
+    int nw = sl.nw;
+#pragma unroll
+    for (int w = 0; w < kStageWin; ++w)
+      wlo[w] = sl.win_lo[w];
+    if constexpr (MULTI) {
+      model_of(j, rp);
+      nw = rnw[rp] < sl.nw ? rnw[rp] : sl.nw;
+#pragma unroll
+      for (int w = 0; w < kStageWin; ++w)
+        wlo[w] = rlo[rp * kStageWin + w];
+    }
     // window w's rows clamped to the vector: [c0, c1)
     auto clamp = [&](int w, long long& c0, long long& c1) {
-      const long long a = first + sl.win_lo[w], b = a + sl.win_rows[w];
+      const long long a = first + wlo[w], b = a + sl.win_rows[w];
       c0 = a > 0 ? a : 0;
       c1 = b < n ? b : n;
     };
@@ -268,7 +322,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     for (int w = 0; w < kStageWin; ++w) {
       long long c0, c1;
       clamp(w, c0, c1);
-      if (w < sl.nw && c1 > c0)
+      if (w < nw && c1 > c0)
         bytes += (unsigned)((c1 - c0) * RB);
     }
     const unsigned tile_bytes = (unsigned)((last - first) * RB);
@@ -279,8 +333,8 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     for (int w = 0; w < kStageWin; ++w) {
       long long c0, c1;
       clamp(w, c0, c1);
-      if (w < sl.nw && c1 > c0)
-        bulk_load(st + sl.win_off[w] + (c0 - (first + sl.win_lo[w])) * RB,
+      if (w < nw && c1 > c0)
+        bulk_load(st + sl.win_off[w] + (c0 - (first + wlo[w])) * RB,
                   t1 + (size_t)c0 * V, (unsigned)((c1 - c0) * RB), full + s);
     }
     if constexpr (MODE == kCheb)
@@ -353,8 +407,12 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     int issued = 0;
     for (int jj = 0; jj < mine; ++jj) {
       const int s = jj % S;
+      if (MULTI && *(volatile int*)&abort_flag)
+        break;
       if (jj >= S && !mbar_wait(empty + s, (unsigned)(jj / S - 1) & 1u)) {
         atomicOr(op.stage_err, 1u);
+        if constexpr (MULTI)
+          *(volatile int*)&abort_flag = 1;
         break;
       }
       fence_async_smem();
@@ -365,26 +423,105 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     for (int jj = issued > S ? issued - S : 0; jj < issued; ++jj)
       mbar_wait(full + jj % S, (unsigned)(jj / S) & 1u);
   }
-  if (compute && mine > 0)
+  // MULTI: the block's sums of model rr, reduced over the compute warps (named barrier 1,
+  // the producer warp takes no part), into the block's slot of that model; the sums
+  // restart from zero.
+  constexpr int kVS = DOT == kDotPair ? 2 * V : V;
+  int rc = -1;           // MULTI: the model whose sums the threads hold
+  unsigned touched = 0;  // MULTI: the models whose slot this block has written
+  auto flush = [&](int rr) {
+    if constexpr (MULTI) {
+      __shared__ double msh[kComputeWarps][kVS][4];
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      constexpr int P = DOT == kDotPair ? 2 : 1;
+      // Two slots at a time, in place (the sums restart from zero afterwards), in the
+      // order of even sites (chunk q, then chunk q + V/4): odd sites hold the halves
+      // swapped.
+      auto put = [&](int k, CSum a, CSum b) {
+#pragma unroll
+        for (int off = 16; off >= kTps; off >>= 1) {
+          csum_merge(a, shfl_xor(a, off));
+          csum_merge(b, shfl_xor(b, off));
+        }
+        if (lane < kTps) {
+          const int v = StageSlots<kHalf, P>{}(lane, k, kSums);
+          msh[warp][v][0] = a.s;
+          msh[warp][v][1] = a.c;
+          msh[warp][v][2] = b.s;
+          msh[warp][v][3] = b.c;
+        }
+      };
+      constexpr int H = kSums / 2;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const CSum a0 = re[k], b0 = im[k], a1 = re[k + H], b1 = im[k + H];
+        re[k] = im[k] = re[k + H] = im[k + H] = CSum{0.0, 0.0};
+        put(k, sw ? a1 : a0, sw ? b1 : b0);
+        put(k + H, sw ? a0 : a1, sw ? b0 : b1);
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(kBlock) : "memory");
+      if (threadIdx.x < kVS) {
+        const int v = threadIdx.x;
+        CSum x{msh[0][v][0], msh[0][v][1]}, y{msh[0][v][2], msh[0][v][3]};
+        for (int w = 1; w < kComputeWarps; ++w) {
+          csum_merge(x, CSum{msh[w][v][0], msh[w][v][1]});
+          csum_merge(y, CSum{msh[w][v][2], msh[w][v][3]});
+        }
+        double* dst = partials + (((size_t)blockIdx.x * R + rr) * kVS + v) * 4;
+        dst[0] = x.s;
+        dst[1] = x.c;
+        dst[2] = y.s;
+        dst[3] = y.c;
+      }
+      asm volatile("bar.sync 1, %0;" ::"n"(kBlock) : "memory");
+      touched |= 1u << rr;
+    }
+  };
+  if (compute && mine > 0) {
     fetch(0, cc, p, la, lb);
+    if constexpr (MULTI) {
+      rc = 0;
+      model_of(0, rc);
+    }
+  }
   for (int j = 0; compute && j < mine; ++j) {
     int cn[Z] = {};
     double pn = 0.0;
     float4 lan = {}, lbn = {};
     if (j + 1 < mine)
       fetch(j + 1, cn, pn, lan, lbn);
+    int cbase = 0;     // MULTI: the model's row of the code table
+    int own = xofs;    // the site's own row in the stage
+    if constexpr (MULTI) {
+      cbase = rc * op.n_codes;
+      own = sl.win_off[0] - rlo[rc * kStageWin] * RB;
+    }
     const int s = j % S;
-    const bool late = !mbar_wait(full + s, (unsigned)(j / S) & 1u);
-    if (__any_sync(0xffffffffu, late)) {
-      if (late)
-        atomicOr(op.stage_err, 1u);
-      break;
+    bool skip = false;
+    if constexpr (MULTI) {
+      // After a wait ran out (in any warp) the block skips its remaining tiles but keeps
+      // taking part in the flushes, so no named barrier waits for a warp that left.
+      const bool stop = *(volatile int*)&abort_flag != 0;
+      const bool late = !stop && !mbar_wait(full + s, (unsigned)(j / S) & 1u);
+      if (__any_sync(0xffffffffu, late)) {
+        if (late)
+          atomicOr(op.stage_err, 1u);
+        *(volatile int*)&abort_flag = 1;
+      }
+      skip = __any_sync(0xffffffffu, stop || late);
+    } else {
+      const bool late = !mbar_wait(full + s, (unsigned)(j / S) & 1u);
+      if (__any_sync(0xffffffffu, late)) {
+        if (late)
+          atomicOr(op.stage_err, 1u);
+        break;
+      }
     }
     const unsigned char* st = stage_smem + (size_t)s * sl.stage_bytes + l * RB;
     const int i = ((int)blockIdx.x + j * G) * TS + l;
-    if (F32 && i < n) {
+    if (!skip && F32 && i < n) {
       float2 x[W];
-      ldsf4(st + xofs, x);
+      ldsf4(st + own, x);
       const float2 pf = split_f32(p * op.inv_emax);
       AccF32 acc[W];
 #pragma unroll
@@ -393,7 +530,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
       for (int m = 0; m < Z; ++m) {
         const int c = cc[m];
-        const int2 ci = cinfo[c];
+        const int2 ci = cinfo[cbase + c];
         const float4 h = hopf[c];
         float2 y[W];
         if (ci.x >= 0) {
@@ -435,9 +572,9 @@ __global__ void __launch_bounds__(kStageThreads, 2)
         }
       }
     }
-    if (!F32 && i < n) {
+    if (!skip && !F32 && i < n) {
       double2 x[W];
-      lds4(st + xofs, x);
+      lds4(st + own, x);
       double tr[W], ti[W];
 #pragma unroll
       for (int k = 0; k < W; ++k) {
@@ -447,7 +584,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
       for (int m = 0; m < Z; ++m) {
         const int c = cc[m];
-        const int2 ci = cinfo[c];
+        const int2 ci = cinfo[cbase + c];
         const double2 h = hop[c];
         double2 y[W];
         if (ci.x >= 0) {
@@ -506,7 +643,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     }
     // this warp has read stage s
     __syncwarp();
-    if ((threadIdx.x & 31) == 0)
+    if (!skip && (threadIdx.x & 31) == 0)
       mbar_arrive(empty + s);
 #pragma unroll
     for (int m = 0; m < Z; ++m)
@@ -514,27 +651,49 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     p = pn;
     la = lan;
     lb = lbn;
-  }
-  // Slots in the order of even sites (chunk q, then chunk q + V/4) on every thread.
-  if (sw) {
-#pragma unroll
-    for (int k = 0; k < kSums / 2; ++k) {
-      const CSum a = re[k], b = im[k];
-      re[k] = re[k + kSums / 2];
-      im[k] = im[k + kSums / 2];
-      re[k + kSums / 2] = a;
-      im[k + kSums / 2] = b;
+    if constexpr (MULTI) {
+      // The block's sums of model rc end with its last tile there. The next tile's model
+      // follows from the tile index alone, so every compute thread flushes in step.
+      int rn = rc;
+      if (j + 1 < mine)
+        model_of(j + 1, rn);
+      if (j + 1 == mine || rn != rc)
+        flush(rc);
+      rc = rn;
     }
   }
-  if constexpr (DOT == kDotLeft)
-    dot_finish_w<V, W, StageSlots<kHalf, 1>, kComputeWarps>(re, im, dot, {});
-  else if constexpr (DOT == kDotPair)
-    dot_finish_w<2 * V, 2 * W, StageSlots<kHalf, 2>, kComputeWarps>(re, im, dot, {});
+  if constexpr (MULTI) {
+    if (compute) {
+      // slots of models this block never met hold zero sums
+      double* slots = partials + (size_t)blockIdx.x * R * kVS * 4;
+      for (int k = threadIdx.x; k < R * kVS * 4; k += kBlock)
+        if (!((touched >> (k / (kVS * 4))) & 1u))
+          slots[k] = 0.0;
+    }
+  } else {
+    // Slots in the order of even sites (chunk q, then chunk q + V/4) on every thread.
+    if (sw) {
+#pragma unroll
+      for (int k = 0; k < kSums / 2; ++k) {
+        const CSum a = re[k], b = im[k];
+        re[k] = re[k + kSums / 2];
+        im[k] = im[k + kSums / 2];
+        re[k + kSums / 2] = a;
+        im[k + kSums / 2] = b;
+      }
+    }
+    if constexpr (DOT == kDotLeft)
+      dot_finish_w<V, W, StageSlots<kHalf, 1>, kComputeWarps>(re, im, dot, {});
+    else if constexpr (DOT == kDotPair)
+      dot_finish_w<2 * V, 2 * W, StageSlots<kHalf, 2>, kComputeWarps>(re, im, dot, {});
+  }
 }
 
 // Stage layout for V vectors over the first nw windows: the windows, then T_{k-2} as
-// the launch needs it; true when at least two stages of it fit.
-bool stage_layout_nw(const Op& op, int V, int mode, int nw, int stages, StageLayout& sl)
+// the launch needs it; true when at least two stages of it fit. budget: the shared memory
+// the stages may take (two blocks per SM).
+bool stage_layout_nw(const Op& op, int V, int mode, int nw, int stages, StageLayout& sl,
+                     int budget)
 {
   const int TS = kBlock * kStageW / V, RB = V * (int)sizeof(float2);
   sl = StageLayout{};
@@ -553,8 +712,8 @@ bool stage_layout_nw(const Op& op, int V, int mode, int nw, int stages, StageLay
   }
   sl.stage_bytes = (off + 127) / 128 * 128;
   if (stages <= 1) {
-    // as many stages as fit 104 KB (two blocks per SM), at most kMaxStages
-    stages = (104 << 10) / sl.stage_bytes;
+    // as many stages as fit the budget, at most kMaxStages
+    stages = budget / sl.stage_bytes;
     stages = stages > kMaxStages ? kMaxStages : stages;
   }
   // at most kMaxStages, and no more than fit 200 KB (a block's shared memory is at most
@@ -568,22 +727,38 @@ bool stage_layout_nw(const Op& op, int V, int mode, int nw, int stages, StageLay
 // The windows come most used first (after the one holding offset 0); when two stages of
 // all of them do not fit, the last ones are left out (their entries gather from global
 // memory) until two do.
-bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayout& sl)
+bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayout& sl,
+                  int budget = 104 << 10)
 {
   (void)dot;  // left never takes shared memory: both moment modes share the layout
   for (int nw = op.stage_nw; nw >= 1; --nw)
-    if (stage_layout_nw(op, V, mode, nw, stages, sl))
+    if (stage_layout_nw(op, V, mode, nw, stages, sl, budget))
       return true;
   return false;
 }
 
-template <int V, int Z, int MODE, int DOT, bool F32>
-gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
-                         const float2* t1, float2* out, const float2* left, const Dot& d)
+// Shared memory a realisation-batch launch of R models takes beside its stages and the
+// one-model tables: the per-model code offsets and window starts, and the block
+// reduction of a model's sums.
+size_t multi_extra_bytes(const Op& op, int R, int V, int dot)
 {
-  auto* kernel = k_step_staged<V, Z, MODE, DOT, F32>;
-  const size_t smem = (size_t)sl.stages * sl.stage_bytes + 2 * kMaxStages * sizeof(uint64_t) +
-                      (size_t)op.n_codes * (sizeof(double2) + sizeof(int2) + sizeof(float4));
+  const int kVS = dot == kDotPair ? 2 * V : V;
+  return (size_t)(R - 1) * op.n_codes * sizeof(int2) + (size_t)R * (kStageWin + 1) * sizeof(int) +
+         (size_t)kComputeWarps * kVS * 4 * sizeof(double);
+}
+
+template <int V, int Z, int MODE, int DOT, bool F32, bool MULTI>
+gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
+                         const float2* t1, float2* out, const float2* left, const Dot& d,
+                         MultiDot md)
+{
+  auto* kernel = k_step_staged<V, Z, MODE, DOT, F32, MULTI>;
+  const int R = MULTI ? md.n_real : 1;
+  size_t smem = (size_t)sl.stages * sl.stage_bytes + 2 * kMaxStages * sizeof(uint64_t) +
+                (size_t)op.n_codes * (sizeof(double2) + sizeof(float4)) +
+                (size_t)R * op.n_codes * sizeof(int2);
+  if (MULTI)
+    smem += (size_t)R * (kStageWin + 1) * sizeof(int);
   static std::mutex mu;
   static std::unordered_map<size_t, int> per_sm;  // blocks per SM by shared memory size
   static size_t attr = 0;                         // the kernel's shared memory limit set
@@ -607,15 +782,23 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
   const int ntiles = (op.n + TS - 1) / TS;
   const int cap = device_info().sms * bps;
   const int grid = ntiles < cap ? ntiles : cap;
-  kernel<<<grid, kStageThreads, smem, stream()>>>(op, sl, t0, t1, out, left, d);
+  if (MULTI) {
+    if (grid > max_grid())
+      return fail(GQT_ERR_STATE, "staged batch step: grid %d above the slot rows", grid);
+    md.blocks = grid;
+    if (md.blocks_out)
+      *md.blocks_out = grid;
+  }
+  kernel<<<grid, kStageThreads, smem, stream()>>>(op, sl, t0, t1, out, left, d, md);
   count_launches(1);
   GQT_CUDA(cudaGetLastError());
   return GQT_OK;
 }
 
-template <int V, bool F32>
+template <int V, bool F32, bool MULTI = false>
 gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, const void* t0,
-                    const void* t1, void* out, const void* left, const Dot& d)
+                    const void* t1, void* out, const void* left, const Dot& d,
+                    const MultiDot& md = MultiDot{})
 {
   const float2* a0 = (const float2*)t0;
   const float2* a1 = (const float2*)t1;
@@ -626,15 +809,16 @@ gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, cons
     if (dot == kDotPair) {
       if constexpr (V <= 16) {
         if (mode == kApply)
-          return launch_staged<V, Z, kApply, kDotPair, F32>(op, sl, a0, a1, o, lf, d);
-        return launch_staged<V, Z, kCheb, kDotPair, F32>(op, sl, a0, a1, o, lf, d);
+          return launch_staged<V, Z, kApply, kDotPair, F32, MULTI>(op, sl, a0, a1, o, lf, d,
+                                                                   md);
+        return launch_staged<V, Z, kCheb, kDotPair, F32, MULTI>(op, sl, a0, a1, o, lf, d, md);
       } else {
         return fail(GQT_ERR_ARG, "symmetric moments: at most 16 vectors per launch");
       }
     }
     if (mode == kApply)
-      return launch_staged<V, Z, kApply, kDotLeft, F32>(op, sl, a0, a1, o, lf, d);
-    return launch_staged<V, Z, kCheb, kDotLeft, F32>(op, sl, a0, a1, o, lf, d);
+      return launch_staged<V, Z, kApply, kDotLeft, F32, MULTI>(op, sl, a0, a1, o, lf, d, md);
+    return launch_staged<V, Z, kCheb, kDotLeft, F32, MULTI>(op, sl, a0, a1, o, lf, d, md);
   };
   switch (op.z) {
     case 3:
@@ -649,10 +833,14 @@ gqt_status staged_v(const Op& op, int mode, int dot, const StageLayout& sl, cons
 }  // namespace
 
 // Whether the staged step serves a step of this operator, vector count and mode, and
-// its layout (the vectors' alignment aside).
-static bool stage_fits(const Op& op, int nvec, int mode, int dot, bool f32, StageLayout& sl)
+// its layout (the vectors' alignment aside). R > 1: a realisation batch of R models
+// (the GQT_FP32R step only).
+static bool stage_fits(const Op& op, int nvec, int mode, int dot, bool f32, StageLayout& sl,
+                       int R = 1)
 {
   if (op.stage_nw <= 0 || !op.code || !op.stage_err || (mode != kApply && mode != kCheb))
+    return false;
+  if ((op.stage_rtab != nullptr) != (R > 1) || (R > 1 && !f32))
     return false;
   // Automatic (0), from B200 measurements with 16 vectors on graphene 2,097,152 sites
   // (rows of 3), square 1024^2 (rows of 4) and cubic 256^3 (rows of 6): the GQT_FP32R
@@ -671,7 +859,10 @@ static bool stage_fits(const Op& op, int nvec, int mode, int dot, bool f32, Stag
     return false;
   if (op.z != 3 && op.z != 4 && op.z != 6)
     return false;
-  return stage_layout(op, nvec, mode, dot, op.stage_stages, sl);
+  int budget = 104 << 10;
+  if (R > 1)
+    budget -= (int)multi_extra_bytes(op, R, nvec, dot);
+  return budget > 0 && stage_layout(op, nvec, mode, dot, op.stage_stages, sl, budget);
 }
 
 bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, const void* t1,
@@ -685,10 +876,10 @@ bool stage_applies(const Op& op, int nvec, int mode, int dot, const void* t0, co
   return stage_fits(op, nvec, mode, dot, f32, sl);
 }
 
-int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows)
+int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows, int R)
 {
   StageLayout sl;
-  const bool on = stage_fits(op, nvec, kCheb, dot, f32, sl);
+  const bool on = stage_fits(op, nvec, kCheb, dot, f32, sl, R);
   if (windows)
     *windows = on ? sl.nw : 0;
   return on ? sl.stages : 0;
@@ -710,6 +901,40 @@ gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
     default:
       return fail(GQT_ERR_ARG, "staged step: unsupported vector count %d", nvec);
   }
+}
+
+// The GQT_FP32R step of a realisation batch (mode kApply or kCheb): the staged step with
+// each model's windows, its sums per (block, model) in md's slots, combined by
+// k_tile_reduce here unless md.defer (then by the caller, over a window of steps).
+gqt_status stage_step_multi(const Op& op, int nvec, int mode, int dot, const void* t0,
+                            const void* t1, void* out, const void* left, const MultiDot& md)
+{
+  auto aligned = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  StageLayout sl;
+  if (!aligned(t1) || !aligned(out) || (mode == kCheb && !aligned(t0)) ||
+      (dot == kDotLeft && !aligned(left)) ||
+      !stage_fits(op, nvec, mode, dot, true, sl, md.n_real))
+    return fail(GQT_ERR_STATE,
+                "the FP32R form runs a realisation batch through its staged step only "
+                "(coded operator, rows of 3, 4 or 6, 16 or 32 vectors, 16 for symmetric "
+                "sets, staging not off); %d vectors here", nvec);
+  MultiDot m = md;
+  int grid = 0;
+  m.blocks_out = &grid;
+  const Dot none{};
+  gqt_status st = GQT_OK;
+  if (nvec == 16)
+    st = staged_v<16, true, true>(op, mode, dot, sl, t0, t1, out, left, none, m);
+  else
+    st = staged_v<32, true, true>(op, mode, dot, sl, t0, t1, out, left, none, m);
+  if (st != GQT_OK)
+    return st;
+  if (md.blocks_out)
+    *md.blocks_out = grid;
+  if (md.defer)
+    return GQT_OK;
+  m.blocks = grid;
+  return forms_fp32(nvec)->fmt[1].tile_reduce(m, dot == kDotPair, 1, 0);
 }
 
 
@@ -844,6 +1069,26 @@ gqt_status step_pair_r(const Op& op, int mode, const void* t0, const void* t1, v
     return run_r<V, kDotPair, C>(op, mode, t0, t1, out, nullptr, d);
 }
 
+// A step of a realisation batch: moment 0 (<left|right> of the stored vectors, the same
+// sums in every FP32 form) through the FP32 form's batch kernel, the others staged.
+template <int V, bool C>
+gqt_status step_multi_r(const Op& op, int mode, const void* t0, const void* t1, void* out,
+                        const void* left, const MultiDot& md, int dot)
+{
+  if (mode == kDotOnly)
+    return forms_fp32(V)->fmt[C ? 1 : 0].step_multi(op, mode, t0, t1, out, left, md, dot);
+  if (!C)
+    return fail(GQT_ERR_STATE, "the FP32R form runs a realisation batch on the coded "
+                               "operator only");
+  return stage_step_multi(op, V, mode, dot, t0, t1, out, left, md);
+}
+
+template <int V>
+gqt_status tile_reduce_r(const MultiDot& md, bool pair, int rows, size_t row_stride)
+{
+  return forms_fp32(V)->fmt[1].tile_reduce(md, pair, rows, row_stride);
+}
+
 template <int V>
 gqt_status dot_r(size_t total, const void* state, const void* left, const Dot& d)
 {
@@ -860,8 +1105,12 @@ const FormOps* table_r()
     f.elem_bytes = sizeof(float2);
     f.fmt[0].step = step_r<V, false>;
     f.fmt[0].step_pair = step_pair_r<V, false>;
+    f.fmt[0].step_multi = step_multi_r<V, false>;
+    f.fmt[0].tile_reduce = tile_reduce_r<V>;
     f.fmt[1].step = step_r<V, true>;
     f.fmt[1].step_pair = step_pair_r<V, true>;
+    f.fmt[1].step_multi = step_multi_r<V, true>;
+    f.fmt[1].tile_reduce = tile_reduce_r<V>;
     f.dot = dot_r<V>;
     return f;
   }();

@@ -56,7 +56,8 @@ enum {
    * hopping and potential divided by energy_max in FP64, then held as two FP32 parts,
    * hi = RN(a) and lo = RN(a - hi)), the Chebyshev recurrence in FP32, and the moments
    * summed in FP64 from the stored FP32 values. Runs on GQT_FP32 vectors as they are,
-   * or on FP32 copies of GQT_FP64 ones. */
+   * or on FP32 copies of GQT_FP64 ones. A realisation batch runs it through the staged
+   * step only (coded operator, 16 or 32 vectors, 16 for symmetric sets). */
   GQT_FP32R = 3
 };
 

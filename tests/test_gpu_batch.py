@@ -116,3 +116,78 @@ def test_batch_tile_sizes_give_the_same_moments(tile):
     assert single.batch_tile == 0
     with pytest.raises(g.GqtError):
         single.set_batch_tile(256)
+
+
+def _pow2_models(tmp_path):
+    """Models whose E_max is a power of two: the batch's pre-divided hoppings h / E_max
+    equal the single model's h * (1 / E_max) bit for bit, so the FP32R arithmetic is the
+    same in both. Square lattices of three sizes (one odd, one with open boundaries and
+    vacancy-free ragged rows) and graphene (rows of 3 padded to 4 in the batch)."""
+    from gpuqt_b200 import workloads as W
+    specs = [("square", (24, 24, 1), -1.0, 2.0, 8.0), ("square", (40, 40, 1), -1.0, 1.0, 8.0),
+             ("square", (17, 17, 1), -1.0, 3.0, 8.0), ("graphene", (8, 4, 1), -2.7, 1.0, 16.0)]
+    out = []
+    for k, (kind, cells, t, w, e) in enumerate(specs):
+        d = W.write_input_dir(str(tmp_path / f"m{k}"), kind, cells, hopping=t, anderson=w,
+                              energy_max=e, moments=160, calculate=(), seed=20 + k)
+        out.append(g.Model.load(d))
+    return out
+
+
+@pytest.mark.parametrize("V", [16, 32])
+def test_batch_fp32r_staged_matches_models_alone(tmp_path, V):
+    """The staged FP32R batch step (each model's own windows, sums flushed per model)
+    against each model run alone in the FP32R form: the same T_m per element, moments
+    to FP64 summation order; the symmetric loop as well (16 vectors)."""
+    models = _pow2_models(tmp_path)
+    B = g.Hamiltonian.batch(models)
+    stages, slots = B.stage_plan(V, g.FP32R)
+    assert stages >= 2 and slots >= 2, (stages, slots)
+    assert B.stage_plan(V, g.FP32) == (0, 0)  # the FP32 form's batch step is not staged
+    ph = _phases(models, V)
+    X = g.Vector.from_host(*B.scatter(ph), nvec=V, precision=g.FP32)
+    M = 160
+    br, bi = g.moments(B, X, X, M, precision=g.FP32R)
+    dr = di = None
+    if V == 16:
+        dr, di = g.moments_doubled(B, X, M, precision=g.FP32R)
+    for r, (m, p) in enumerate(zip(models, ph)):
+        H = g.Hamiltonian(m)
+        x = g.Vector.from_host(p[0], p[1], nvec=V, precision=g.FP32)
+        sr, si = g.moments(H, x, x, M, precision=g.FP32R)
+        scale = float(np.max(np.hypot(sr, si)))
+        assert float(np.max(np.hypot(br[r] - sr, bi[r] - si))) <= 1e-12 * scale, r
+        if V == 16:
+            sr, si = g.moments_doubled(H, x, M, precision=g.FP32R)
+            assert float(np.max(np.hypot(dr[r] - sr, di[r] - si))) <= 1e-12 * scale, r
+
+
+def test_batch_fp32r_dos_close_to_fp64():
+    models = _models()
+    B = g.Hamiltonian.batch(models)
+    V = 16
+    ph = _phases(models, V)
+    X32 = g.Vector.from_host(*B.scatter(ph), nvec=V, precision=g.FP32)
+    M = 200
+    r32, i32 = g.moments(B, X32, X32, M, precision=g.FP32R)
+    for r, m in enumerate(models):
+        H = g.Hamiltonian(m)
+        x = g.Vector.from_host(ph[r][0][0], ph[r][1][0])
+        r64, i64 = g.moments(H, x, x, M)
+        d64 = g.chebyshev_summation(r64, i64, m.energy, m.energy_max, m.volume)
+        d32 = g.chebyshev_summation(r32[r, 0], i32[r, 0], m.energy, m.energy_max, m.volume)
+        bound = 2e-6 if NAMES[r] == "graphene_8x4" else 1e-6  # few sharp levels
+        assert np.max(np.abs(d32 - d64)) <= bound * np.max(np.abs(d64)), r
+
+
+def test_batch_fp32r_needs_the_staged_step():
+    models = _models()[:2]
+    B = g.Hamiltonian.batch(models)
+    X = g.Vector(B.n, nvec=16, precision=g.FP32)
+    B.set_staging(-1)
+    with pytest.raises(g.GqtError):
+        g.moments(B, X, X, 10, precision=g.FP32R)
+    B.set_staging(0)
+    B.set_format(g.FORMAT_ELL)
+    with pytest.raises(g.GqtError):
+        g.moments(B, X, X, 10, precision=g.FP32R)

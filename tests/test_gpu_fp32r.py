@@ -118,11 +118,7 @@ def test_fp32r_limits():
     X32 = g.Vector.from_host(*_states(m, 32), nvec=32, precision=g.FP32)
     with pytest.raises(g.GqtError):
         g.moments_doubled(H, X32, 10, precision=g.FP32R)  # at most 16 for symmetric sets
-    models = [g.Model.load(fixture_dir(n)) for n in ("sq16_pbc", "cubic6")]
-    B = g.Hamiltonian.batch(models)
-    XB = g.Vector(B.n, nvec=16, precision=g.FP32)
-    with pytest.raises(g.GqtError):
-        g.moments(B, XB, XB, 10, precision=g.FP32R)
+    # realisation batches: tests/test_gpu_batch.py
 
 
 def test_fp32r_at_size(tmp_path):
