@@ -225,16 +225,19 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   double2* hop = reinterpret_cast<double2*>(empty + kMaxStages);
   // GQT_FP32R: the hoppings divided by E_max as FP32 (hi, lo) parts
   float4* hopf = reinterpret_cast<float4*>(hop + op.n_codes);
-  // per code (MULTI: per model and code): byte offset in a stage of site 0's neighbour
-  // row (-1: gathered from global memory), and the offset j - i
+  // per code: byte offset in a stage of site 0's neighbour row (-1: gathered from global
+  // memory), and the offset j - i. MULTI: the byte offsets per model and code (coff) and
+  // the offsets j - i per code (cdelta) instead.
   int2* cinfo = reinterpret_cast<int2*>(hopf + op.n_codes);
+  int* coff = reinterpret_cast<int*>(hopf + op.n_codes);
   // MULTI: md's fields as values (lambdas then capture no kernel parameter by address)
   const int R = MULTI ? md.n_real : 1;
   const int* const tile_first = md.tile_first;
   const long long tile_sites = md.tile_sites;
   double* const partials = md.partials;
+  int* cdelta = coff + (size_t)R * op.n_codes;
   // MULTI: each model's window starts [R][kStageWin], then its window count [R]
-  int* rlo = reinterpret_cast<int*>(cinfo + (size_t)R * op.n_codes);
+  int* rlo = cdelta + op.n_codes;
   const int* rnw = rlo + R * kStageWin;
   __shared__ int abort_flag;  // MULTI: a wait ran out; the block computes no further
 
@@ -255,6 +258,8 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     const int* tab = op.stage_rtab;
     for (int k = threadIdx.x; k < R * (kStageWin + 1); k += blockDim.x)
       rlo[k] = tab[k];
+    for (int c = threadIdx.x; c < op.n_codes; c += blockDim.x)
+      cdelta[c] = op.code_delta[c];
     const int* slot = tab + R * (kStageWin + 1);
     for (int k = threadIdx.x; k < R * op.n_codes; k += blockDim.x) {
       const int r = k / op.n_codes, d = op.code_delta[k % op.n_codes], w = slot[k];
@@ -265,7 +270,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
       for (int q = 0; q < kStageWin; ++q)
         if (q == w && q < sl.nw)
           o = sl.win_off[q] + (d - tab[r * kStageWin + q]) * RB;
-      cinfo[k] = make_int2(o, d);
+      coff[k] = o;
     }
   }
   if (threadIdx.x == 0) {
@@ -530,7 +535,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
       for (int m = 0; m < Z; ++m) {
         const int c = cc[m];
-        const int2 ci = cinfo[cbase + c];
+        const int2 ci = MULTI ? make_int2(coff[cbase + c], cdelta[c]) : cinfo[c];
         const float4 h = hopf[c];
         float2 y[W];
         if (ci.x >= 0) {
@@ -584,7 +589,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
 #pragma unroll
       for (int m = 0; m < Z; ++m) {
         const int c = cc[m];
-        const int2 ci = cinfo[cbase + c];
+        const int2 ci = MULTI ? make_int2(coff[cbase + c], cdelta[c]) : cinfo[c];
         const double2 h = hop[c];
         double2 y[W];
         if (ci.x >= 0) {
@@ -737,14 +742,29 @@ bool stage_layout(const Op& op, int V, int mode, int dot, int stages, StageLayou
   return false;
 }
 
-// Shared memory a realisation-batch launch of R models takes beside its stages and the
-// one-model tables: the per-model code offsets and window starts, and the block
-// reduction of a model's sums.
-size_t multi_extra_bytes(const Op& op, int R, int V, int dot)
+// Dynamic shared memory of a launch beside its stages: the barriers, the hopping table in
+// FP64 and FP32 parts and the code offsets (R > 1, a realisation batch of R models: per
+// model and code, with the offsets j - i per code and each model's window starts).
+size_t stage_table_bytes(const Op& op, int R)
+{
+  const size_t base = 2 * kMaxStages * sizeof(uint64_t) +
+                      (size_t)op.n_codes * (sizeof(double2) + sizeof(float4));
+  if (R <= 1)
+    return base + (size_t)op.n_codes * sizeof(int2);
+  return base + ((size_t)R * op.n_codes + op.n_codes + (size_t)R * (kStageWin + 1)) * sizeof(int);
+}
+
+// The stages' share of a realisation-batch launch: the one-model budget less what the
+// batch adds, the per-model tables and the block reduction of a model's sums (static,
+// kComputeWarps x the model's sums x 32 B). On the 8-model benchmark batch that leaves
+// two stages. Three fit two blocks per SM too (112 KB each), but measured on B200 they
+// ran the symmetric loop at 1.99e11 site-moments/s against 2.49e11 with two, and the
+// direct loop at the same rate.
+int multi_stage_budget(const Op& op, int R, int V, int dot)
 {
   const int kVS = dot == kDotPair ? 2 * V : V;
-  return (size_t)(R - 1) * op.n_codes * sizeof(int2) + (size_t)R * (kStageWin + 1) * sizeof(int) +
-         (size_t)kComputeWarps * kVS * 4 * sizeof(double);
+  const int added = (int)stage_table_bytes(op, R) - (int)stage_table_bytes(op, 1);
+  return (104 << 10) - added - kComputeWarps * kVS * 4 * (int)sizeof(double);
 }
 
 template <int V, int Z, int MODE, int DOT, bool F32, bool MULTI>
@@ -754,11 +774,7 @@ gqt_status launch_staged(const Op& op, const StageLayout& sl, const float2* t0,
 {
   auto* kernel = k_step_staged<V, Z, MODE, DOT, F32, MULTI>;
   const int R = MULTI ? md.n_real : 1;
-  size_t smem = (size_t)sl.stages * sl.stage_bytes + 2 * kMaxStages * sizeof(uint64_t) +
-                (size_t)op.n_codes * (sizeof(double2) + sizeof(float4)) +
-                (size_t)R * op.n_codes * sizeof(int2);
-  if (MULTI)
-    smem += (size_t)R * (kStageWin + 1) * sizeof(int);
+  const size_t smem = (size_t)sl.stages * sl.stage_bytes + stage_table_bytes(op, R);
   static std::mutex mu;
   static std::unordered_map<size_t, int> per_sm;  // blocks per SM by shared memory size
   static size_t attr = 0;                         // the kernel's shared memory limit set
@@ -859,9 +875,7 @@ static bool stage_fits(const Op& op, int nvec, int mode, int dot, bool f32, Stag
     return false;
   if (op.z != 3 && op.z != 4 && op.z != 6)
     return false;
-  int budget = 104 << 10;
-  if (R > 1)
-    budget -= (int)multi_extra_bytes(op, R, nvec, dot);
+  const int budget = R > 1 ? multi_stage_budget(op, R, nvec, dot) : (104 << 10);
   return budget > 0 && stage_layout(op, nvec, mode, dot, op.stage_stages, sl, budget);
 }
 
