@@ -134,6 +134,7 @@ Op make_op(const gqt_ham* h, int nvec = 1)
   op.nl = h->nl;
   op.hop = h->hop;
   op.pot = h->pot;
+  op.pot_r = h->pot_r;
   op.xx = h->xx;
   op.emax = h->energy_max;
   op.inv_emax = 1.0 / h->energy_max;
@@ -871,6 +872,8 @@ static gqt_status moments_run(const gqt_ham* h, const gqt_vec* left, const gqt_v
   if (!mu_dev)
     return fail(GQT_ERR_ARG, "%s: null output", w);
   Workspace& ws = *h->ws;
+  if (right->precision == GQT_FP32R)
+    GQT_TRY(ensure_pot_r(h));  // before any capture: it allocates
   if (wave_eligible(h, right, pair)) {
     GQT_TRY(wave_prepare(h, ws));
     if (h->wave_halo >= 0)

@@ -128,6 +128,8 @@ gqt_status stage_step(const Op& op, int nvec, int mode, int dot, const void* t0,
 // for nvec vectors (dot kDotLeft: direct, kDotPair: symmetric sets); 0 when it would not
 // be staged.
 int stage_plan(const Op& op, int nvec, int dot, bool f32, int* windows, int R = 1);
+// The FP32R form's split potential of h (gqt_ham::pot_r), made on first use.
+gqt_status ensure_pot_r(const gqt_ham* h);
 // Grid size for a grid-stride kernel: enough blocks to cover `total` elements, capped
 // at the number of blocks that are resident at once on all SMs.
 int grid_for(const void* kernel, size_t total);

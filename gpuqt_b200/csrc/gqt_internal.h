@@ -82,6 +82,9 @@ struct gqt_ham {
   double2* hop = nullptr;   // [z*n] column-major
   double* xx = nullptr;     // [z*n] column-major
   double* pot = nullptr;    // [n]
+  // [n]: the FP32R form's (hi, lo) FP32 parts of pot * RN(1 / energy_max), made on that
+  // form's first use with the kernels' own arithmetic (null until then)
+  mutable float2* pot_r = nullptr;
   bool has_xx = false;
   // Coded operator (built when the (j - i, hopping, xx) entries of the ELL take at
   // most GQT_MAX_CODES distinct values, as lattice models do): one byte per entry and

@@ -41,6 +41,7 @@ struct Op {
   const int* __restrict__ nl;
   const double2* __restrict__ hop;
   const double* __restrict__ pot;
+  const float2* __restrict__ pot_r;  // the FP32R form's split potential (gqt_ham::pot_r)
   const double* __restrict__ xx;
   double emax;
   double inv_emax;  // RN(1 / emax)

@@ -435,6 +435,7 @@ gqt_ham::~gqt_ham()
   cudaFree(hop);
   cudaFree(xx);
   cudaFree(pot);
+  cudaFree(pot_r);
   cudaFree(tile_first_all);  // tile_first points into it
   cudaFree(code);
   cudaFree(code_delta);

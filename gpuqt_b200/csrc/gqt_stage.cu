@@ -385,13 +385,17 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   // codes, potential and (moment <left|T_k>) this thread's left chunks of tile j's
   // site l, loaded one tile ahead into registers: left is read only by the moment, so
   // it takes no shared memory
-  auto fetch = [&](int j, int (&c)[Z], double& p, float4& la, float4& lb) {
+  // (GQT_FP32R: the potential's FP32 parts pr, made once per operator; GQT_FP32: p)
+  auto fetch = [&](int j, int (&c)[Z], double& p, float2& pr, float4& la, float4& lb) {
     const int i = ((int)blockIdx.x + j * G) * TS + l;
     if (i < n) {
 #pragma unroll
       for (int m = 0; m < Z; ++m)
         c[m] = op.code[(size_t)m * n + i];
-      p = op.pot[i];
+      if constexpr (F32)
+        pr = op.pot_r[i];
+      else
+        p = op.pot[i];
       if constexpr (DOT == kDotLeft && F32) {
         const float4* row = reinterpret_cast<const float4*>(left + (size_t)i * V);
         la = __ldg(row + ca);
@@ -401,6 +405,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   };
   int cc[Z] = {};
   double p = 0.0;
+  float2 pr = {};
   float4 la = {}, lb = {};
   // Warps 0 .. kComputeWarps - 1 compute; thread kBlock (the next warp) issues the copies.
   // A compute warp waits for a stage's full barrier and, once its lanes have read the
@@ -483,7 +488,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     }
   };
   if (compute && mine > 0) {
-    fetch(0, cc, p, la, lb);
+    fetch(0, cc, p, pr, la, lb);
     if constexpr (MULTI) {
       rc = 0;
       model_of(0, rc);
@@ -492,9 +497,10 @@ __global__ void __launch_bounds__(kStageThreads, 2)
   for (int j = 0; compute && j < mine; ++j) {
     int cn[Z] = {};
     double pn = 0.0;
+    float2 prn = {};
     float4 lan = {}, lbn = {};
     if (j + 1 < mine)
-      fetch(j + 1, cn, pn, lan, lbn);
+      fetch(j + 1, cn, pn, prn, lan, lbn);
     int cbase = 0;     // MULTI: the model's row of the code table
     int own = xofs;    // the site's own row in the stage
     if constexpr (MULTI) {
@@ -527,7 +533,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     if (!skip && F32 && i < n) {
       float2 x[W];
       ldsf4(st + own, x);
-      const float2 pf = split_f32(p * op.inv_emax);
+      const float2 pf = pr;
       AccF32 acc[W];
 #pragma unroll
       for (int k = 0; k < W; ++k)
@@ -654,6 +660,7 @@ __global__ void __launch_bounds__(kStageThreads, 2)
     for (int m = 0; m < Z; ++m)
       cc[m] = cn[m];
     p = pn;
+    pr = prn;
     la = lan;
     lb = lbn;
     if constexpr (MULTI) {
@@ -955,6 +962,32 @@ gqt_status stage_step_multi(const Op& op, int nvec, int mode, int dot, const voi
 // ------------------------------------------------------------------ the GQT_FP32R form
 namespace {
 
+// The potential divided by E_max as FP32 (hi, lo) parts, as the steps used to form it
+// per element: split_f32(pot * RN(1 / E_max)).
+__global__ void __launch_bounds__(kBlock) k_split_pot(const double* __restrict__ pot,
+                                                      double inv_emax, float2* out, int n)
+{
+  for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock)
+    out[i] = split_f32(pot[i] * inv_emax);
+}
+
+}  // namespace
+
+gqt_status ensure_pot_r(const gqt_ham* h)
+{
+  if (h->pot_r)
+    return GQT_OK;
+  GQT_CUDA(cudaMalloc(&h->pot_r, (size_t)h->n * sizeof(float2)));
+  const int grid = (h->n + kBlock - 1) / kBlock < max_grid() ? (h->n + kBlock - 1) / kBlock
+                                                             : max_grid();
+  k_split_pot<<<grid, kBlock, 0, stream()>>>(h->pot, 1.0 / h->energy_max, h->pot_r, h->n);
+  count_launches(1);
+  GQT_CUDA(cudaGetLastError());
+  return GQT_OK;
+}
+
+namespace {
+
 // The GQT_FP32R step without staging (the ELL arrays, operators without windows, vectors
 // not on 16-byte boundaries): grid-stride items of one site and 4 consecutive vectors,
 // with the staged step's arithmetic (entries past a row's length are skipped).
@@ -994,7 +1027,7 @@ __global__ void __launch_bounds__(kBlock, r_min_blocks<Z>()) k_step_r(Op op, con
     const size_t base = (size_t)i * V + (size_t)(g % kTps) * W;
     float2 x[W];
     ld4(t1 + base, x);
-    const float2 pf = split_f32(op.pot[i] * op.inv_emax);
+    const float2 pf = op.pot_r[i];
     AccF32 acc[W];
 #pragma unroll
     for (int k = 0; k < W; ++k)

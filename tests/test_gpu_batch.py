@@ -191,3 +191,33 @@ def test_batch_fp32r_needs_the_staged_step():
     B.set_format(g.FORMAT_ELL)
     with pytest.raises(g.GqtError):
         g.moments(B, X, X, 10, precision=g.FP32R)
+
+
+def test_batch_fp32r_staged_many_models(tmp_path):
+    """32 square lattices (the most a batch takes) of 16^2 to 47^2 sites, each padded to
+    1024 sites: a block's tiles fall in many models, with models skipped between them
+    (their slots zeroed), and the sums are flushed at every model change. Against each
+    model run alone in the FP32R form (E_max a power of two: the same operator)."""
+    from gpuqt_b200 import workloads as W
+    models = []
+    for k in range(32):
+        L = 16 + k
+        d = W.write_input_dir(str(tmp_path / f"m{k}"), "square", (L, L, 1), hopping=-1.0,
+                              anderson=0.5 + 0.1 * k, energy_max=8.0, moments=64,
+                              calculate=(), seed=100 + k)
+        models.append(g.Model.load(d))
+    B = g.Hamiltonian.batch(models)
+    V, M = 16, 64
+    assert B.stage_plan(V, g.FP32R)[0] >= 2
+    ph = _phases(models, V)
+    X = g.Vector.from_host(*B.scatter(ph), nvec=V, precision=g.FP32)
+    br, bi = g.moments(B, X, X, M, precision=g.FP32R)
+    dr, di = g.moments_doubled(B, X, M, precision=g.FP32R)
+    for r, (m, p) in enumerate(zip(models, ph)):
+        H = g.Hamiltonian(m)
+        x = g.Vector.from_host(p[0], p[1], nvec=V, precision=g.FP32)
+        sr, si = g.moments(H, x, x, M, precision=g.FP32R)
+        scale = float(np.max(np.hypot(sr, si)))
+        assert float(np.max(np.hypot(br[r] - sr, bi[r] - si))) <= 1e-12 * scale, r
+        sr, si = g.moments_doubled(H, x, M, precision=g.FP32R)
+        assert float(np.max(np.hypot(dr[r] - sr, di[r] - si))) <= 1e-12 * scale, r
