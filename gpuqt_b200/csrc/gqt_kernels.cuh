@@ -970,10 +970,18 @@ __device__ __forceinline__ void step_dot(CSum (&re)[2], CSum (&im)[2], double2 o
 // registers between near-identical builds of the same loop. The pair mode on the ELL
 // arrays (hoppings travelling with the prefetched row, two compensated products) takes
 // 2: at 3 it spilled 50-180 bytes per thread.
+// GQT_STEP_BLOCKS_ROWS6 (compile time, default 2) sets the budget for rows of six: at 3
+// (80 registers, 80 bytes spilled) the FP64 step ran 13-21 % slower on B200 (cubic slab
+// 32x256x256: 4.9e10 against 5.7e10 site-moments/s; cubic 256^3: 4.6e10 against 5.9e10).
+#ifndef GQT_STEP_BLOCKS_ROWS6
+#define GQT_STEP_BLOCKS_ROWS6 2
+#endif
 template <int Z, int DOT = kDotLeft, bool C = true>
 constexpr int step_min_blocks()
 {
-  return (Z >= 6 || (DOT == kDotPair && !C)) ? 2 : 3;
+  if constexpr (DOT == kDotPair && !C)
+    return 2;
+  return Z >= 6 ? GQT_STEP_BLOCKS_ROWS6 : 3;
 }
 
 template <typename VT2, int V, int Z, class A, int MODE, int DOT, bool C>
