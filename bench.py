@@ -13,7 +13,7 @@ Also reported, on the same line:
   e2e           the same metric through the public API with host buffers
   forms         graphene 2M in every form: FP64 on the ELL arrays, FP32 storage with
                 1/16/32 vectors per launch, symmetric (doubled) sets in FP64 and FP32,
-                each with its byte model and roofline fraction; `north_star` states the
+                each with its byte model and roofline fraction; `target_ratios` states the
                 FP32/FP64 ratios like for like (direct/direct, doubled/doubled) next to
                 their byte-model ceilings
   evolution     the Bessel evolution of one 1 fs MSD step (evolve, evolvex)
@@ -691,7 +691,7 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
                       "frac": ach / hbm_peak,
                       "bytes_per_site_moment": fp64_bytes_per_site(coded=coded)}
 
-    # The north-star ratio, like for like: batched FP32 storage over plain FP64 in the
+    # The target ratio, like for like: batched FP32 storage over plain FP64 in the
     # same loop (direct over direct, doubled over doubled), each next to the ratio of
     # the two forms' byte models, which bounds it while both are HBM-bound.
     d32 = out["fp32_v16"]
@@ -700,7 +700,7 @@ def measure_forms(g, torch, m, H, phi, args, stream, hbm_peak):
                 fp32_pair_bytes_per_site_vector_step(16, coded=coded))
     ratio_direct = d32["site_moments_per_s"] / rate64
     ratio_dbl = rate32_dbl / rate64_dbl
-    out["north_star"] = {
+    out["target_ratios"] = {
         "target": "batched FP32 >= 3x plain FP64 site-moments/s, both >= 0.70 of HBM "
                   "roofline, <= 1e-6 error",
         "speedup_direct": ratio_direct, "byte_ceiling_direct": ceil_direct,

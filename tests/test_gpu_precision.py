@@ -4,7 +4,7 @@ graphene, 4,194,304 sites, W = 1.5, seed 5, 5000 moments), DOS and all 20 VAC st
 The error measures, per moment set (precision_report.compare):
   energy_rel_peak_max     max over energies |X32(E) - X64(E)| / max_E |X64(E)|, the
                           norm-wise relative error of the DOS or VAC row; bound 1e-6
-                          for the DOS and every VAC step
+                          (the target tolerance) for the DOS and every VAC step
   energy_rel_in_band_max  max |X32(E) - X64(E)| / |X64(E)| over energies where
                           |X64(E)| > 1 % of the row's peak (pointwise); bound 1e-6 for
                           the DOS. For the VAC at late correlation times the row is a
