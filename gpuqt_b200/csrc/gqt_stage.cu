@@ -176,11 +176,13 @@ __device__ __forceinline__ void cmac_f32(AccF32& a, float4 h, float2 y)
 
 // One part of T_k = 2 (hi + lo) - T_{k-2} with a single rounding of the hi sum: 2 hi -
 // T_{k-2} is split exactly into s + e (Knuth's TwoSum; 2 hi is exact), then 2 lo and e
-// are added to s. Rounding hi + lo first leaves an error of the order of hi's last
-// place, and hi is near T_{k-2} / 2 where T_k is small: in a model of the recurrence
-// (graphene, 2000 moments) that rounding gave 14x the moment error of this form, 23x that
-// of the FP32 form. Explicit round-to-nearest intrinsics keep the compiler from fusing
-// the sequence.
+// are added to s. The lo accumulator is below half an ulp of hi (as the operator's lo
+// parts are below half an ulp of theirs), so RN(hi + lo) is hi: rounding that sum first
+// dropped the lo parts and applied H rounded to FP32, a fixed perturbation of H whose
+// error grows with the moment index. Adding 2 lo after rounding 2 hi - T_{k-2} drops
+// them wherever T_{k-2} sets the scale. In a model of the recurrence (graphene, 2000
+// moments) those finishes gave 14x and 7x the moment error of this one. Explicit
+// round-to-nearest intrinsics keep the compiler from fusing the sequence.
 __device__ __forceinline__ float cheb_part(float hi, float lo, float y0)
 {
   const float s = __fmaf_rn(2.0f, hi, -y0);
