@@ -176,10 +176,10 @@ __device__ __forceinline__ void cmac_f32(AccF32& a, float4 h, float2 y)
 
 // One part of T_k = 2 (hi + lo) - T_{k-2} with a single rounding of the hi sum: 2 hi -
 // T_{k-2} is split exactly into s + e (Knuth's TwoSum; 2 hi is exact), then 2 lo and e
-// are added to s. The lo accumulator is below half an ulp of hi (as the operator's lo
-// parts are below half an ulp of theirs), so RN(hi + lo) is hi: rounding that sum first
-// dropped the lo parts and applied H rounded to FP32, a fixed perturbation of H whose
-// error grows with the moment index. Adding 2 lo after rounding 2 hi - T_{k-2} drops
+// are added to s. The lo accumulator is mostly below half an ulp of hi (each lo part
+// of the operator is below half an ulp of its hi part), so RN(hi + lo) is mostly hi:
+// rounding that sum first dropped the lo parts and applied H rounded to FP32, a fixed
+// perturbation of H whose error grows with the moment index. Adding 2 lo after rounding 2 hi - T_{k-2} drops
 // them wherever T_{k-2} sets the scale. In a model of the recurrence (graphene, 2000
 // moments) those finishes gave 14x and 7x the moment error of this one. Explicit
 // round-to-nearest intrinsics keep the compiler from fusing the sequence.
