@@ -188,6 +188,9 @@ def test_batch_fp32r_needs_the_staged_step():
     with pytest.raises(g.GqtError):
         g.moments(B, X, X, 10, precision=g.FP32R)
     B.set_staging(0)
+    X32 = g.Vector(B.n, nvec=32, precision=g.FP32)
+    with pytest.raises(g.GqtError):  # symmetric sets: at most 16 vectors per launch
+        g.moments_doubled(B, X32, 10, precision=g.FP32R)
     B.set_format(g.FORMAT_ELL)
     with pytest.raises(g.GqtError):
         g.moments(B, X, X, 10, precision=g.FP32R)
