@@ -1,5 +1,6 @@
 // Test infrastructure only (never linked into the product): a driver that links the
-// reference's own CPU objects (src/*.cu built with -DCPU_ONLY -DDEBUG, see Makefile)
+// reference's own CPU objects (src/*.cu built with -DCPU_ONLY -DDEBUG, see Makefile), or
+// its GPU objects (target ref_gpu, the same source compiled by nvcc),
 // and writes their raw results at full precision, so the parity tests can pin the
 // C restatement (lsqt_oracle.c) and the CUDA library against the reference itself.
 //
@@ -214,6 +215,9 @@ int main(int argc, char** argv)
     for (int r = 0; r < reps; ++r) {
       auto t0 = std::chrono::steady_clock::now();
       find_moments_chebyshev(model, H, phi, phi, out);
+#ifdef __CUDACC__
+      cudaDeviceSynchronize();  // the GPU build's launches are asynchronous
+#endif
       auto t1 = std::chrono::steady_clock::now();
       std::printf("%s%.6f", r ? ", " : "", std::chrono::duration<double>(t1 - t0).count());
       std::fflush(stdout);
