@@ -1011,7 +1011,11 @@ def measure_batch(g, torch, tmp, stream, hbm_peak, vectors=64, moments=2000):
                 "dos_err_vs_fp64": dos_error(g, m0, (r64, i64), (qr[0, 0], qi[0, 0])),
                 "stages": stages, "window_slots": slots}
 
-    fp32r_direct = fp32r(32, False) if B.format == g.FORMAT_CODED else None
+    fp32r_direct = None
+    if B.format == g.FORMAT_CODED:
+        # the vectors per launch as the autotuner picks them for this form
+        vr, vr_rates = g.autotune_nvec(B, g.FP32R, 20, [16, 32])
+        fp32r_direct = dict(fp32r(vr, False), autotune_rates=vr_rates)
     fp32r_doubled = fp32r(16, True) if B.format == g.FORMAT_CODED else None
     return {"realisations": [[m.n, round(m.energy_max, 4)] for m in models],
             "doubled": {"site_moments_per_s": vectors * sites * moments / (dbl_ms / 1e3),

@@ -1419,7 +1419,8 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
     if (form_ops(precision, V)) {
       gqt_vec* x = nullptr;
       double2* mu = nullptr;
-      st = gqt_vec_create(h->n, V, precision, &x);
+      // GQT_FP32R probes run on FP32 vectors (the form's storage)
+      st = gqt_vec_create(h->n, V, precision == GQT_FP32R ? GQT_FP32 : precision, &x);
       if (st == GQT_OK) {
         const size_t bytes = (size_t)n_moments * h->n_real * V * sizeof(double2);
         cudaError_t ce = cudaMalloc(&mu, bytes);
@@ -1430,23 +1431,27 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
       // realisation batch, each with every tile size.
       const int shapes[2] = {0, 2};
       const int n_shapes = (precision == GQT_FP32 && V >= 4) ? 2 : 1;
-      const int n_tiles = h->n_real > 1 ? kBatchTiles : 1;
+      // (the FP32R batch step hands out its own tiles: the batch tile does not apply)
+      const int n_tiles = (h->n_real > 1 && precision != GQT_FP32R) ? kBatchTiles : 1;
       int best_w = 0, best_t = h->tile_sites;
       for (int q = 0; q < n_shapes * n_tiles && st == GQT_OK; ++q) {
         const int si = q / n_tiles;
-        h->wpt[V] = shapes[si];
+        // the vectors-per-thread shape is the FP32 form's (FP32R leaves it as it is)
+        if (precision != GQT_FP32R)
+          h->wpt[V] = shapes[si];
         if (h->n_real > 1) {
           st = batch_set_tile(const_cast<gqt_ham*>(h), kBatchTileSizes[q % n_tiles]);
           if (st != GQT_OK)
             break;
         }
-        st = gqt_moments_device(h, x, x, n_moments, mu);  // warm-up, graph capture
+        // warm-up, graph capture
+        st = gqt_moments_device_form(h, x, x, n_moments, precision, mu);
         float ms = 0.f;
         if (st == GQT_OK) {
           cudaEventRecord(e0, s);
-          st = gqt_moments_device(h, x, x, n_moments, mu);
+          st = gqt_moments_device_form(h, x, x, n_moments, precision, mu);
           if (st == GQT_OK)
-            st = gqt_moments_device(h, x, x, n_moments, mu);
+            st = gqt_moments_device_form(h, x, x, n_moments, precision, mu);
           cudaEventRecord(e1, s);
           cudaError_t ce = cudaEventSynchronize(e1);
           if (ce == cudaSuccess)
@@ -1473,9 +1478,11 @@ extern "C" gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_m
           }
         }
       }
-      if (h->wpt[V] != best_w || n_shapes > 1 || n_tiles > 1)
-        changed = true;
-      h->wpt[V] = best_w;
+      if (precision != GQT_FP32R) {
+        if (h->wpt[V] != best_w || n_shapes > 1 || n_tiles > 1)
+          changed = true;
+        h->wpt[V] = best_w;
+      }
       if (rate > best_rate)
         best_tile = best_t;
       cudaFree(mu);

@@ -188,7 +188,9 @@ gqt_status gqt_ham_realisation(const gqt_ham* h, int r, int* offset, int* n,
  * (rates[k] receives candidate k's best rate; may be NULL). For every candidate it
  * also picks the vector-block shape of the step (vectors per thread, FP32: 4 or 2)
  * and, on a realisation batch, the tile size (256, 512 or 1024 sites), keeping the
- * fastest for later launches. Allocates and frees its own probe vectors. */
+ * fastest for later launches. GQT_FP32R is probed on FP32 vectors with its own staged
+ * tiles (on a batch its candidates are 16 and 32). Allocates and frees its own probe
+ * vectors. */
 gqt_status gqt_autotune_nvec(const gqt_ham* h, int precision, int n_moments,
                              const int* candidates, int n_candidates, int* best,
                              double* rates);

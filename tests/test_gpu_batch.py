@@ -224,3 +224,16 @@ def test_batch_fp32r_staged_many_models(tmp_path):
         assert float(np.max(np.hypot(br[r] - sr, bi[r] - si))) <= 1e-12 * scale, r
         sr, si = g.moments_doubled(H, x, M, precision=g.FP32R)
         assert float(np.max(np.hypot(dr[r] - sr, di[r] - si))) <= 1e-12 * scale, r
+
+
+def test_autotuner_probes_the_fp32r_batch():
+    """The autotuner runs the FP32R form on FP32 probe vectors and picks one of the
+    candidates it could time; the batch then runs with it."""
+    models = _models()
+    B = g.Hamiltonian.batch(models)
+    best, rates = g.autotune_nvec(B, g.FP32R, 10, [16, 32])
+    assert best in (16, 32) and all(rates[v] > 0 for v in (16, 32)), rates
+    X = g.Vector(B.n, nvec=best, precision=g.FP32)
+    X.upload(*B.scatter(_phases(models, best)))
+    r, i = g.moments(B, X, X, 20, precision=g.FP32R)
+    assert np.all(np.isfinite(r)) and np.all(np.isfinite(i))
