@@ -131,6 +131,14 @@ void run(Model& model, long long max_rows, int precision)
   if (model.batch_vectors > 1 && ckpt)
     throw InputError("batch_vectors cannot be combined with checkpoints (checkpoint_every, "
                      "a bounded run): checkpoints are per row of one vector");
+  // The FP32R moment form launches 4, 16 or 32 vectors at a time: every moment set must
+  // come from a group of 16 or 4 (the LDOS runs one orbital vector at a time).
+  if (precision == GQT_FP32R &&
+      (model.batch_vectors < 4 || model.number_of_random_vectors % 4 != 0 ||
+       model.calculate_ldos))
+    throw InputError("the FP32R moment form runs groups of 4 or 16 vectors: set batch_vectors "
+                     "4 or 16, a number_of_random_vectors divisible by 4, and no local "
+                     "orbitals (the LDOS runs one vector at a time)");
   Hamiltonian H(model);
   Vector random_state(model.number_of_atoms);
   const bool v = model.verbose;
@@ -345,7 +353,7 @@ extern "C" gqt_status gqt_lsqt_run(const char* dir, int precision, int verbose,
     *finished = 0;
   if (!dir)
     return GQT_ERR_ARG;
-  if (precision != GQT_FP64 && precision != GQT_FP32)
+  if (precision != GQT_FP64 && precision != GQT_FP32 && precision != GQT_FP32R)
     return GQT_ERR_ARG;
   const int saved = Vector::moment_precision;
   gqt_host::ThrowScope scope;

@@ -1,5 +1,5 @@
 // lsqt_b200: drop-in for the reference's lsqt_gpu / lsqt_cpu binaries
-// (src/main.cu:34-56). Usage: lsqt_b200 input.txt [--fp32]
+// (src/main.cu:34-56). Usage: lsqt_b200 input.txt [--fp32 | --fp32r]
 // input.txt lists one input directory per line; each is run with lsqt().
 #include <chrono>
 #include <cstring>
@@ -20,13 +20,15 @@ int main(int argc, char* argv[])
   for (int i = 1; i < argc; ++i) {
     if (std::strcmp(argv[i], "--fp32") == 0)
       Vector::moment_precision = GQT_FP32;
+    else if (std::strcmp(argv[i], "--fp32r") == 0)
+      Vector::moment_precision = GQT_FP32R;  // needs batch_vectors 4 or 16
     else if (!driver)
       driver = argv[i];
     else
       driver = nullptr, i = argc;
   }
   if (!driver) {
-    std::cout << "Usage: lsqt_b200 input.txt [--fp32]" << std::endl;
+    std::cout << "Usage: lsqt_b200 input.txt [--fp32 | --fp32r]" << std::endl;
     return 1;
   }
   std::ifstream input(driver);

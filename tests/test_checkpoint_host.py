@@ -87,3 +87,14 @@ def test_moments_reader(tmp_path):
         f.write(b"\0" * 8)
     with pytest.raises(ValueError):
         g.read_moments(p)
+
+
+@pytest.mark.parametrize("extra", ["", "batch_vectors 4\n"])
+def test_fp32r_run_needs_groups_of_four(tmp_path, extra):
+    """The FP32R moment form launches 4, 16 or 32 vectors: a run without groups, or with
+    a vector count (2 here) that leaves a smaller group, is refused before any device
+    work."""
+    d = _dir(tmp_path, extra)
+    with pytest.raises(g.GqtError) as e:
+        g.lsqt(d, precision=g.FP32R)
+    assert e.value.status == 4 and "FP32R" in str(e.value), str(e.value)

@@ -76,6 +76,19 @@ def test_groups_with_doubling_and_fp32(tmp_path):
     assert _same_outputs(a, c, tol=1e-6) >= 4
 
 
+def test_groups_in_the_fp32r_form(tmp_path):
+    """The FP32R moment form (FP32 vectors and hoppings, the recurrence in FP32) on the
+    groups: every .out row within 1e-6 of its peak of the FP64 run's, with the direct
+    and with the symmetric (kpm_doubling) moment loop."""
+    extra = "number_of_random_vectors 4\n"
+    a = _run(tmp_path, "sq16_pbc", "_seq", extra)
+    b = _run(tmp_path, "sq16_pbc", "_f32r", extra + "batch_vectors 4\n", precision=g.FP32R)
+    assert _same_outputs(a, b, tol=1e-6) >= 4
+    c = _run(tmp_path, "sq16_pbc", "_f32rd", extra + "batch_vectors 16\nkpm_doubling\n",
+             precision=g.FP32R)
+    assert _same_outputs(a, c, tol=1e-6) >= 4
+
+
 def test_groups_refuse_checkpoints(tmp_path):
     d = str(tmp_path / "ck")
     shutil.copytree(fixture_dir("chain_z2"), d)
