@@ -344,7 +344,9 @@ gqt_status gqt_model_initial_state(gqt_model* m, int orbital, double* re, double
 /* Replaces lsqt(std::string) (src/lsqt.cu:135-152): the full run for one input
  * directory, appending dos.out / vac0.out / vac.out / msd.out / S.out / ldos.out
  * with the reference's formats. precision selects the arithmetic form of the moment
- * recurrence; states and their time evolution stay FP64. */
+ * recurrence (GQT_FP64, GQT_FP32, or GQT_FP32R, which needs batch_vectors 4 or 16, a
+ * number of random vectors divisible by 4 and no local orbitals); states and their
+ * time evolution stay FP64. */
 gqt_status gqt_lsqt(const char* input_dir, int precision, int verbose);
 /* gqt_lsqt with checkpoint / resume; no counterpart in the reference. A checkpoint
  * (input_dir/lsqt.checkpoint: the next row's position, the generator state, the
