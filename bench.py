@@ -363,6 +363,10 @@ def run_ours(args):
     from gpuqt_b200 import workloads as W
 
     rank, world, local = dist()
+    if world > 1:
+        # The forms, batch, cubic and precision sections characterise one GPU (the N = 1
+        # run reports them); a run over N replicas measures the scaled loop alone.
+        args.no_forms = args.no_batch = args.no_cubic = args.no_precision = True
     hbm_peak, peak_kind = peaks()
     tmp = tempfile.mkdtemp(prefix=f"gqt_bench_{rank}_")
     try:
